@@ -1,0 +1,198 @@
+/* taral_pdhg.h -- C ABI of the B200 PDHG engine for continuous LPs (sm_100a).
+ *
+ * Drop-in boundary for the TARAL-LP PDHG path. Three layers, each replacing a reference interface:
+ *
+ *   1. Backend concept (pdhg_*): the eight methods the reference's driver template calls on a backend,
+ *      gpu/pdhg.cu:313-514 (struct Gpu<T>) and :583-741 (struct Cpu<T>), over an opaque device context.
+ *   2. Solver entry (taral_pdhg_solve): the reference's whole solve path for one model -- input gate
+ *      (gpu/pdhg_input.hpp:7-26), scaling (gpu/pdhg.cu:80-133), driver run<B>() (gpu/pdhg.cu:761-849) and the
+ *      original-space check of finish() (gpu/pdhg.cu:858-911).
+ *   3. Problem format (taral_mps_*): the reference's MPS reader, src/mps.cpp:96-399 / src/taral.hpp:48,
+ *      returning a model with the semantics of Model (src/taral.hpp:22-35).
+ *
+ * Conventions
+ *   - Every call returns an int status: TARAL_OK (0) or a negative TARAL_ERR_*; the reference exits the
+ *     process on any CUDA error (gpu/pdhg.cu:36-43) where this ABI returns TARAL_ERR_CUDA instead.
+ *     pdhg_last_error() gives the message of the last failure on a context.
+ *   - Host arrays passed in are read during the call only (copied); the context owns all device memory and
+ *     its CUDA stream. One host thread per context; contexts are independent of each other.
+ *   - Reductions are fixed-order: the same input gives bit-identical results on the same GPU.
+ *   - Indices are 0-based; row/column pointer arrays are int64; infinite bounds are +-INFINITY.
+ */
+#ifndef TARAL_PDHG_H
+#define TARAL_PDHG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TARAL_PDHG_ABI_VERSION 1
+
+enum taral_status {
+    TARAL_OK = 0,
+    TARAL_ERR_CUDA = -1,        /* a CUDA runtime call failed (message in pdhg_last_error) */
+    TARAL_ERR_ALLOC = -2,       /* device or host allocation failed */
+    TARAL_ERR_INPUT = -3,       /* malformed arguments (sizes, pointers, index ranges) */
+    TARAL_ERR_UNSUPPORTED = -4, /* integer or quadratic model (gpu/pdhg_input.hpp:7-17) */
+    TARAL_ERR_PARSE = -5,       /* MPS file could not be read */
+    TARAL_ERR_STATE = -6,       /* call out of order (e.g. iterate before start) */
+    TARAL_ERR_NO_DEVICE = -7    /* no CUDA device, or not an sm_100 part */
+};
+
+/* Arithmetic of the iteration. FP64: everything in double (the reference's default).
+ * FP32: matrix values, iterates x, z and the products Ax, A^T z in float; running averages, KKT
+ * residuals, gap, restart tests and the primal weight in double. */
+enum taral_precision { TARAL_FP64 = 0, TARAL_FP32 = 1 };
+
+/* pdhg_create flags */
+#define TARAL_FLAG_NO_GRAPH 1u /* launch each block's kernels directly instead of replaying a CUDA graph */
+
+/* Row-wise CSR in host memory. ptr has rows+1 entries; column indices ascending within a row. */
+typedef struct {
+    int rows, cols;
+    int64_t nnz;
+    const int64_t* ptr;
+    const int32_t* idx;
+    const double* val;
+} taral_csr;
+
+/* ------------------------------------------------------------------------------------------------------------
+ * 1. Backend concept. Replaces Gpu<T> (gpu/pdhg.cu:313-514). All vectors are in the SCALED space of
+ *    gpu/pdhg.cu:72-78: A_s = diag(Dr) A diag(Dc), c_s = Dc c, [l,u]_s = [l,u]/Dc, [rl,ru]_s = Dr [rl,ru].
+ * ------------------------------------------------------------------------------------------------------------ */
+typedef struct pdhg_ctx pdhg_ctx;
+
+/* Gpu::init (gpu/pdhg.cu:362-382): upload A and A^T (AT must be the transpose of A), the 7 vectors and
+ * allocate the iteration state on the current CUDA device. eval_freq = steps per captured graph (64). */
+int pdhg_create(const taral_csr* A, const taral_csr* AT, const double* c, const double* l, const double* u,
+                const double* rl, const double* ru, const double* Dr, const double* Dc, int m, int n,
+                int precision, int eval_freq, unsigned flags, pdhg_ctx** out);
+/* Gpu::power_norm (gpu/pdhg.cu:416-436): sigma_max(A_s) by power iteration on A_s^T A_s, at most iters
+ * steps, stopping after step 10 once the estimate changes by <= 1e-7 relative. */
+int pdhg_power_norm(pdhg_ctx* ctx, int iters, double* norm_out);
+/* Gpu::set_steps (gpu/pdhg.cu:442-445): primal step tau, dual step sigma. */
+int pdhg_set_steps(pdhg_ctx* ctx, double tau, double sigma);
+/* Gpu::start (gpu/pdhg.cu:450-458): x0 = clamp(0, l, u) when x0 is NULL, z0 = 0 when z0 is NULL (a warm start
+ * passes both); x_last = x0, z_last = z0; averages cleared; Ax and A^T z recomputed exactly. */
+int pdhg_start(pdhg_ctx* ctx, const double* x0, const double* z0);
+/* Gpu::iterate (gpu/pdhg.cu:459-486): `steps` PDHG iterations; a block of exactly eval_freq steps replays a
+ * CUDA graph captured on first use. Asynchronous: returns once the work is queued on the context stream. */
+int pdhg_iterate(pdhg_ctx* ctx, int steps);
+/* Gpu::eval (gpu/pdhg.cu:487-499): the 10 FP64 KKT scalars of the current point (avg = 0) or of the running
+ * average scaled by f (avg = 1), in the order {PR2S, PR2O, PR2R, DROW, DZ2, DR2S, DR2O, POBJ, DCOL, DX2}
+ * (gpu/pdhg.cu:136, 145). Synchronises the context stream. */
+int pdhg_eval(pdhg_ctx* ctx, int avg, double f, double out[10]);
+/* Both evaluations of one block (current, then average scaled by f) with one synchronisation. */
+int pdhg_eval_pair(pdhg_ctx* ctx, double f, double cur[10], double avg[10]);
+/* Gpu::restart (gpu/pdhg.cu:500-504): restart to the average scaled by f (avg = 1) or to the current point. */
+int pdhg_restart(pdhg_ctx* ctx, int avg, double f);
+/* Gpu::download (gpu/pdhg.cu:505-513): x (n) and z (m) of the current point or of the scaled average, FP64. */
+int pdhg_download(pdhg_ctx* ctx, int avg, double f, double* x, double* z);
+/* Gpu::name / Gpu::mem_used. name_out receives at most cap bytes (NUL-terminated). */
+int pdhg_info(pdhg_ctx* ctx, char* name_out, size_t cap, size_t* mem_used);
+/* Total kernels this context has launched (graph replays count their kernels). */
+int64_t pdhg_kernel_launches(const pdhg_ctx* ctx);
+const char* pdhg_last_error(const pdhg_ctx* ctx);
+void pdhg_destroy(pdhg_ctx* ctx);
+
+/* ------------------------------------------------------------------------------------------------------------
+ * 2. Solver entry. Replaces main() -> build_scaled -> solve_with<T> -> run<Gpu<T>> -> finish
+ *    (gpu/pdhg.cu:937-992, :913-935, :761-849, :858-911) for a model already in memory.
+ * ------------------------------------------------------------------------------------------------------------ */
+
+/* Column-wise model with the semantics of Model (src/taral.hpp:22-35). is_int may be NULL (all continuous);
+ * n_quadratic is the number of nonzero quadratic objective terms (0 for an LP). */
+typedef struct {
+    int m, n;
+    const int64_t* col_ptr; /* n+1 */
+    const int32_t* row_idx; /* nnz, rows ascending within each column */
+    const double* val;      /* nnz */
+    const double *cost, *col_lo, *col_up, *row_lo, *row_up;
+    double obj_const;
+    int maximize;
+    const unsigned char* is_int;
+    int64_t n_quadratic;
+} taral_model;
+
+/* Options (gpu/pdhg.cu:744-750) plus the precision switch of the CLI's --fp32. */
+typedef struct {
+    double tol;         /* 1e-4 */
+    double time_limit;  /* seconds, 3600 */
+    int64_t max_iter;   /* 2e9 */
+    int eval_freq;      /* 64 */
+    double row_rel;     /* 0 = off */
+    int verbose;        /* 0 */
+    int graph;          /* 1 */
+    int precision;      /* TARAL_FP64 */
+} taral_options;
+
+enum taral_solve_status { TARAL_NEAR_OPTIMAL = 0, TARAL_ITERATION_LIMIT = 1, TARAL_TIME_LIMIT = 2,
+                          TARAL_NUMERICAL_FAILURE = 3 };
+
+/* Outcome (gpu/pdhg.cu:752-759) and the figures finish() prints (gpu/pdhg.cu:866-897). */
+typedef struct {
+    int status;             /* taral_solve_status */
+    int64_t iterations;
+    int restarts;
+    int from_average;       /* 1: the answer is the running average, 0: the current iterate */
+    double rel_primal, rel_dual, rel_gap;
+    double norm_a, primal_weight;
+    double objective;       /* model sense, including obj_const */
+    double max_row_violation, max_bound_violation; /* original model, absolute */
+    double scale_s, device_init_s, transfer_s, solve_s, power_iter_s;
+    size_t device_mem_bytes;
+    int64_t kernel_launches;
+    int64_t nnz;
+} taral_outcome;
+
+void taral_options_default(taral_options* o);
+/* pdhg_input_error (gpu/pdhg_input.hpp:7-17): NULL for a continuous LP, else the rejection reason. */
+const char* taral_pdhg_input_error(const taral_model* md);
+/* Solve one LP. x_out (n, original space) and y_out (m, y = Dr z, minimisation form) may be NULL.
+ * Returns TARAL_ERR_UNSUPPORTED (with nothing computed) for integer or quadratic models. */
+int taral_pdhg_solve(const taral_model* md, const taral_options* o, taral_outcome* out, double* x_out,
+                     double* y_out);
+/* taral_pdhg_solve from a given start point instead of x = clamp(0, l, u), y = 0: x0 (n, original space) and y0
+ * (m, minimisation-form row multipliers, as written by --dual) are scaled into the solver's space. Either may be
+ * NULL. This is the warm-start hook of the learned initialiser; the reference has no counterpart (its only
+ * restart across solves is the simplex crossover of src/crossover.cpp:15-60). */
+int taral_pdhg_solve_warm(const taral_model* md, const taral_options* o, const double* x0, const double* y0,
+                          taral_outcome* out, double* x_out, double* y_out);
+
+/* ------------------------------------------------------------------------------------------------------------
+ * 3. Problem format. Replaces read_mps (src/taral.hpp:48, src/mps.cpp:388-399): free format first, fixed
+ *    columns as fallback; RANGES, OBJSENSE, bound types, integer markers and quadratic sections are read;
+ *    |bound| >= 1e20 is infinite. The handle owns the arrays its model view points into.
+ * ------------------------------------------------------------------------------------------------------------ */
+typedef struct taral_mps taral_mps;
+/* On TARAL_ERR_PARSE, *out is NULL and taral_mps_error() returns the parser's message. */
+int taral_mps_read(const char* path, taral_mps** out);
+const char* taral_mps_error(void);
+int taral_mps_model(const taral_mps* h, taral_model* view);
+const char* taral_mps_col_name(const taral_mps* h, int j);
+const char* taral_mps_row_name(const taral_mps* h, int i);
+const char* taral_mps_name(const taral_mps* h);
+void taral_mps_free(taral_mps* h);
+
+/* ------------------------------------------------------------------------------------------------------------
+ * 4. Standalone CSR SpMV on device buffers. Replaces the warp-per-row kernel of gpu/csr_matvec.cu:23-32:
+ *    y = A x for a CSR matrix already resident on the device (int32 ptr/idx; float or double values and
+ *    vectors). A plan holds the row-block partition of the matrix, built once from the host ptr array.
+ * ------------------------------------------------------------------------------------------------------------ */
+typedef struct taral_spmv_plan taral_spmv_plan;
+/* dtype: TARAL_FP64 (double val/x/y) or TARAL_FP32 (float val/x/y, FP64 accumulation). */
+int taral_spmv_plan_create(int rows, int cols, const int64_t* host_ptr, int dtype, taral_spmv_plan** out);
+/* d_ptr (rows+1 int32), d_idx (nnz int32), d_val, d_x, d_y: device pointers (16-byte aligned idx/val take the
+ * vector-load path); stream: a cudaStream_t, or NULL for the legacy default stream. Asynchronous. */
+int taral_spmv_run(const taral_spmv_plan* plan, const int32_t* d_ptr, const int32_t* d_idx, const void* d_val,
+                   const void* d_x, void* d_y, void* stream);
+int taral_spmv_plan_blocks(const taral_spmv_plan* plan);
+void taral_spmv_plan_destroy(taral_spmv_plan* plan);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TARAL_PDHG_H */

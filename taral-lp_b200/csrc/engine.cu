@@ -1,0 +1,524 @@
+// Device context of the B200 PDHG engine and the C ABI of its backend concept (include/taral_pdhg.h, part 1 and 4).
+//
+// HBM layout of one context (T = double for TARAL_FP64, float for TARAL_FP32):
+//   A   (m rows): ptr int32[m+1], idx int32[nnz], val T[nnz], row blocks int32[nblk+1]
+//   A^T (n rows): the same for the transposed copy (products with A^T never use atomics)
+//   data   c, l, u, Dc : T[n]        rl, ru, Dr : T[m]        par : T[2] = {tau, sigma}
+//   state  x, ATz, xlast : T[n]      z, Ax, zlast : T[m]      xs : f64[n]  zs : f64[m]  (running sums)
+//   eval   tmp_n f64[n], tmp_m f64[m] (products of the sums), partials, tickets, 20 result doubles
+// The running sums of A x and A^T z that the reference keeps (gpu/pdhg.cu:188, :200) are not stored: the
+// average's products are formed once per evaluation as A xs and A^T zs, which saves 16 bytes of state traffic
+// per row and per column every iteration.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/taral_pdhg.h"
+#include "engine.hpp"
+#include "kernels.cuh"
+
+namespace taral {
+
+// ---------------------------------------------------------------------------------------------- row blocks
+std::vector<int> build_row_blocks(const int64_t* ptr, int rows) {
+    std::vector<int> b{0};
+    int cur_rows = 0;
+    int64_t cur_nnz = 0;
+    for (int r = 0; r < rows; ++r) {
+        int64_t L = ptr[r + 1] - ptr[r];
+        if (L > kTile) {  // a long row is a block of its own
+            if (cur_rows) b.push_back(r), cur_rows = 0, cur_nnz = 0;
+            b.push_back(r + 1);
+            continue;
+        }
+        if (cur_rows == kRowsMax || cur_nnz + L > kTile) b.push_back(r), cur_rows = 0, cur_nnz = 0;
+        ++cur_rows, cur_nnz += L;
+    }
+    if (cur_rows) b.push_back(rows);
+    return b;
+}
+
+static int grid_for(int64_t k) {  // elementwise kernels: grid-stride, at most 8 CTAs of 256 per SM
+    return int(std::max<int64_t>(1, std::min<int64_t>((k + 255) / 256, 148 * 8)));
+}
+static int red_grid(int64_t k) {  // reductions: fixed grid per size, so the partial-sum order is fixed
+    return int(std::max<int64_t>(1, std::min<int64_t>((k + 255) / 256, 296)));
+}
+
+struct CudaError {
+    std::string msg;
+};
+#define CK(call)                                                                                           \
+    do {                                                                                                   \
+        cudaError_t e_ = (call);                                                                           \
+        if (e_ != cudaSuccess)                                                                             \
+            throw CudaError{std::string(#call) + ": " + cudaGetErrorString(e_) + " (" + __FILE__ + ":" +   \
+                            std::to_string(__LINE__) + ")"};                                               \
+    } while (0)
+
+struct DevMat {
+    int rows = 0;
+    int64_t nnz = 0;
+    int *ptr = nullptr, *idx = nullptr, *blk = nullptr;
+    void* val = nullptr;
+    int nblk = 0;
+};
+
+template <class T>
+struct Engine final : EngineBase {
+    int m = 0, n = 0, eval_freq = 64;
+    bool use_graph = true;
+    DevMat A, AT;
+    T *c = nullptr, *l = nullptr, *u = nullptr, *rl = nullptr, *ru = nullptr, *Dr = nullptr, *Dc = nullptr,
+      *par = nullptr;
+    T *x = nullptr, *z = nullptr, *Ax = nullptr, *ATz = nullptr, *xlast = nullptr, *zlast = nullptr;
+    T *pv = nullptr, *pw = nullptr, *pu = nullptr;
+    double *xs = nullptr, *zs = nullptr, *tmp_m = nullptr, *tmp_n = nullptr, *hbuf = nullptr, *part = nullptr,
+           *out = nullptr, *pst = nullptr, *h_out = nullptr, *d_in = nullptr;
+    unsigned* tickets = nullptr;
+    int* pdone = nullptr;
+    int* h_flag = nullptr;
+    cudaStream_t st = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    std::vector<void*> allocs;
+    bool started = false;
+
+    template <class U>
+    U* alloc(size_t count) {
+        void* p = nullptr;
+        cudaError_t e = cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(U));
+        if (e != cudaSuccess) throw CudaError{std::string("cudaMalloc: ") + cudaGetErrorString(e)};
+        allocs.push_back(p);
+        return static_cast<U*>(p);
+    }
+    T* upload(const double* v, size_t k) {
+        std::vector<T> h(v, v + k);
+        T* p = alloc<T>(k);
+        if (k) CK(cudaMemcpyAsync(p, h.data(), k * sizeof(T), cudaMemcpyHostToDevice, st));
+        CK(cudaStreamSynchronize(st));
+        return p;
+    }
+    template <class U>
+    U* zeros(size_t k) {
+        U* p = alloc<U>(k);
+        CK(cudaMemsetAsync(p, 0, std::max<size_t>(k, 1) * sizeof(U), st));
+        return p;
+    }
+    DevMat upload(const taral_csr& a) {
+        DevMat d;
+        d.rows = a.rows, d.nnz = a.nnz;
+        std::vector<int> p32(size_t(a.rows) + 1);
+        for (int r = 0; r <= a.rows; ++r) p32[r] = int(a.ptr[r]);
+        std::vector<int> blk = build_row_blocks(a.ptr, a.rows);
+        d.nblk = int(blk.size()) - 1;
+        d.ptr = alloc<int>(p32.size()), d.idx = alloc<int>(size_t(a.nnz)), d.blk = alloc<int>(blk.size());
+        CK(cudaMemcpyAsync(d.ptr, p32.data(), p32.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+        if (a.nnz) CK(cudaMemcpyAsync(d.idx, a.idx, size_t(a.nnz) * sizeof(int), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(d.blk, blk.data(), blk.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+        d.val = upload(a.val, size_t(a.nnz));
+        return d;
+    }
+
+    void init(const taral_csr& hA, const taral_csr& hAT, const double* hc, const double* hl, const double* hu,
+              const double* hrl, const double* hru, const double* hDr, const double* hDc, int m_, int n_,
+              int freq, unsigned flags) {
+        m = m_, n = n_, eval_freq = std::max(1, freq), use_graph = !(flags & TARAL_FLAG_NO_GRAPH);
+        size_t free0, free1, total;
+        CK(cudaMemGetInfo(&free0, &total));
+        int dev;
+        CK(cudaGetDevice(&dev));
+        cudaDeviceProp prop;
+        CK(cudaGetDeviceProperties(&prop, dev));
+        name = prop.name;
+        CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        A = upload(hA), AT = upload(hAT);
+        c = upload(hc, n), l = upload(hl, n), u = upload(hu, n), Dc = upload(hDc, n);
+        rl = upload(hrl, m), ru = upload(hru, m), Dr = upload(hDr, m);
+        par = zeros<T>(2);
+        x = zeros<T>(n), ATz = zeros<T>(n), xlast = zeros<T>(n);
+        z = zeros<T>(m), Ax = zeros<T>(m), zlast = zeros<T>(m);
+        xs = zeros<double>(n), zs = zeros<double>(m), tmp_n = zeros<double>(n), tmp_m = zeros<double>(m);
+        pv = zeros<T>(n), pw = zeros<T>(m), pu = zeros<T>(n);
+        hbuf = alloc<double>(size_t(std::max(m, n)));
+        d_in = alloc<double>(size_t(std::max(m, n)));
+        part = zeros<double>(size_t(296) * 5 * 2);
+        out = zeros<double>(32);
+        pst = zeros<double>(4);
+        tickets = zeros<unsigned>(4);
+        pdone = zeros<int>(1);
+        CK(cudaMallocHost(&h_out, 32 * sizeof(double)));
+        CK(cudaMallocHost(&h_flag, sizeof(int)));
+        CK(cudaStreamSynchronize(st));
+        CK(cudaMemGetInfo(&free1, &total));
+        mem_used = free0 - free1;
+    }
+    ~Engine() override {
+        if (graph) cudaGraphExecDestroy(graph);
+        if (st) cudaStreamSynchronize(st);
+        for (void* p : allocs) cudaFree(p);
+        if (h_out) cudaFreeHost(h_out);
+        if (h_flag) cudaFreeHost(h_flag);
+        if (st) cudaStreamDestroy(st);
+    }
+
+    // ------------------------------------------------------------------ SpMV-shaped launches
+    template <class X, class E>
+    void rowblock(const DevMat& a, const X* xin, const E& epi, const int* skip = nullptr) {
+        if (a.nblk == 0) return;
+        k_rowblock<T, X, E, true><<<a.nblk, kThreads, 0, st>>>(a.ptr, a.idx, static_cast<const T*>(a.val), xin,
+                                                                a.blk, skip, epi);
+        ++launches;
+    }
+    template <class X, class Y>
+    void spmv(const DevMat& a, const X* xin, Y* y, const int* skip = nullptr) {
+        rowblock(a, xin, EpiStore<Y>{y}, skip);
+    }
+    void products() {  // Ax = A x, ATz = A^T z exactly (gpu/pdhg.cu:446-449)
+        spmv(A, x, Ax);
+        spmv(AT, z, ATz);
+    }
+
+    // ------------------------------------------------------------------ backend concept
+    double power_norm(int iters) override {
+        std::vector<double> h(n);
+        double nn = 0;
+        for (int j = 0; j < n; ++j) h[j] = 0.5 + double((uint32_t(j) * 2654435761u) % 1000u) / 1000.0, nn += h[j] * h[j];
+        for (int j = 0; j < n; ++j) h[j] = h[j] / std::sqrt(nn);
+        if (n) CK(cudaMemcpyAsync(d_in, h.data(), size_t(n) * sizeof(double), cudaMemcpyHostToDevice, st));
+        k_cast<T><<<grid_for(n), 256, 0, st>>>(n, d_in, pv);
+        CK(cudaMemsetAsync(pst, 0, 4 * sizeof(double), st));
+        CK(cudaMemsetAsync(pdone, 0, sizeof(int), st));
+        launches += 1;
+        T *a = pv, *b = pu;
+        const int chunk = 8;  // steps queued between checks of the device-side stop flag
+        for (int it = 0; it < iters;) {
+            int end = std::min(iters, it + chunk);
+            for (; it < end; ++it) {
+                spmv(A, a, pw, pdone);
+                spmv(AT, pw, b, pdone);
+                int g = red_grid(n);
+                k_power_sumsq<T><<<g, kRedThreads, 0, st>>>(n, b, part, tickets + 2, out + 24, pdone);
+                k_power_update<<<1, 1, 0, st>>>(out + 24, pst, pdone, it);
+                k_power_scale<T><<<grid_for(n), 256, 0, st>>>(n, b, pst, pdone);
+                launches += 3;
+                std::swap(a, b);
+            }
+            CK(cudaMemcpyAsync(h_flag, pdone, sizeof(int), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            if (*h_flag) break;
+        }
+        CK(cudaMemcpyAsync(h_out, pst, sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        CK(cudaGetLastError());
+        return h_out[0];
+    }
+    void set_steps(double tau, double sigma) override {
+        k_set_par<T><<<1, 1, 0, st>>>(par, T(tau), T(sigma));
+        ++launches;
+        CK(cudaGetLastError());
+    }
+    void start(const double* x0, const double* z0) override {
+        if (x0) {
+            CK(cudaMemcpyAsync(d_in, x0, size_t(n) * sizeof(double), cudaMemcpyHostToDevice, st));
+            k_set_point<T><<<grid_for(n), 256, 0, st>>>(n, d_in, x, xlast, xs);
+        } else {
+            k_start_x<T><<<grid_for(n), 256, 0, st>>>(n, l, u, x, xlast, xs);
+        }
+        ++launches;
+        if (z0) {  // the copy into d_in above has been consumed in stream order before this one lands
+            CK(cudaMemcpyAsync(d_in, z0, size_t(m) * sizeof(double), cudaMemcpyHostToDevice, st));
+            k_set_point<T><<<grid_for(m), 256, 0, st>>>(m, d_in, z, zlast, zs);
+        } else {
+            k_zero_point<T><<<grid_for(m), 256, 0, st>>>(m, z, zlast, zs);
+        }
+        ++launches;
+        products();
+        CK(cudaStreamSynchronize(st));
+        CK(cudaGetLastError());
+        started = true;
+    }
+    void launch_block(int steps) {
+        k_xupd<T><<<grid_for(n), 256, 0, st>>>(n, x, ATz, c, l, u, par, xs);
+        for (int s = 0; s < steps; ++s) {
+            rowblock(A, x, EpiRow<T>{Ax, z, zs, rl, ru, par});
+            rowblock(AT, z, EpiCol<T>{ATz, x, xs, c, l, u, par, s + 1 < steps ? 1 : 0});
+        }
+    }
+    void iterate(int steps) override {
+        if (steps <= 0) return;
+        if (use_graph && steps == eval_freq) {
+            if (!graph) {
+                cudaGraph_t g;
+                int64_t before = launches;
+                CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+                launch_block(steps);
+                CK(cudaStreamEndCapture(st, &g));
+                CK(cudaGraphInstantiate(&graph, g, 0));
+                CK(cudaGraphDestroy(g));
+                launches = before;
+            }
+            CK(cudaGraphLaunch(graph, st));
+            launches += 1 + 2 * int64_t(steps);
+        } else {
+            launch_block(steps);
+            launches += 1;
+        }
+        CK(cudaGetLastError());
+    }
+    void queue_eval(bool avg, double f, double* dst) {
+        int gr = red_grid(m), gc = red_grid(n);
+        if (!avg) {
+            k_eval_row<T, T><<<gr, kRedThreads, 0, st>>>(m, 1.0 * f, Ax, z, rl, ru, Dr, zlast, part, tickets, dst);
+            k_eval_col<T, T><<<gc, kRedThreads, 0, st>>>(n, 1.0 * f, x, ATz, c, l, u, Dc, xlast, part + 296 * 5,
+                                                          tickets + 1, dst + 5);
+        } else {
+            spmv(A, xs, tmp_m);
+            spmv(AT, zs, tmp_n);
+            k_eval_row<T, double><<<gr, kRedThreads, 0, st>>>(m, f, tmp_m, zs, rl, ru, Dr, zlast, part, tickets, dst);
+            k_eval_col<T, double><<<gc, kRedThreads, 0, st>>>(n, f, xs, tmp_n, c, l, u, Dc, xlast, part + 296 * 5,
+                                                               tickets + 1, dst + 5);
+        }
+        launches += 2;
+    }
+    void eval(bool avg, double f, double* o10) override {
+        queue_eval(avg, f, out);
+        CK(cudaMemcpyAsync(h_out, out, 10 * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        CK(cudaGetLastError());
+        std::memcpy(o10, h_out, 10 * sizeof(double));
+    }
+    void eval_pair(double f, double* cur, double* avg) override {
+        queue_eval(false, 1.0, out);
+        queue_eval(true, f, out + 10);
+        CK(cudaMemcpyAsync(h_out, out, 20 * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        CK(cudaGetLastError());
+        std::memcpy(cur, h_out, 10 * sizeof(double));
+        std::memcpy(avg, h_out + 10, 10 * sizeof(double));
+    }
+    void restart(bool avg, double f) override {
+        k_restart<T><<<grid_for(n), 256, 0, st>>>(n, avg ? 1 : 0, f, x, xs, xlast);
+        k_restart<T><<<grid_for(m), 256, 0, st>>>(m, avg ? 1 : 0, f, z, zs, zlast);
+        launches += 2;
+        products();
+        CK(cudaGetLastError());
+    }
+    void download(bool avg, double f, double* hx, double* hz) override {
+        if (n) {
+            if (avg) k_scale_out<double><<<grid_for(n), 256, 0, st>>>(n, f, xs, hbuf);
+            else k_scale_out<T><<<grid_for(n), 256, 0, st>>>(n, 1.0, x, hbuf);
+            CK(cudaMemcpyAsync(hx, hbuf, size_t(n) * sizeof(double), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+        }
+        if (m) {
+            if (avg) k_scale_out<double><<<grid_for(m), 256, 0, st>>>(m, f, zs, hbuf);
+            else k_scale_out<T><<<grid_for(m), 256, 0, st>>>(m, 1.0, z, hbuf);
+            CK(cudaMemcpyAsync(hz, hbuf, size_t(m) * sizeof(double), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+        }
+        launches += 2;
+        CK(cudaGetLastError());
+    }
+    void sync() override { CK(cudaStreamSynchronize(st)); }
+};
+
+std::unique_ptr<EngineBase> make_engine(int precision) {
+    if (precision == TARAL_FP32) return std::make_unique<Engine<float>>();
+    return std::make_unique<Engine<double>>();
+}
+
+void engine_init(EngineBase& e, int precision, const taral_csr& A, const taral_csr& AT, const double* c,
+                 const double* l, const double* u, const double* rl, const double* ru, const double* Dr,
+                 const double* Dc, int m, int n, int freq, unsigned flags) {
+    if (precision == TARAL_FP32)
+        static_cast<Engine<float>&>(e).init(A, AT, c, l, u, rl, ru, Dr, Dc, m, n, freq, flags);
+    else
+        static_cast<Engine<double>&>(e).init(A, AT, c, l, u, rl, ru, Dr, Dc, m, n, freq, flags);
+}
+
+std::string cuda_error_message(const void* exc) { return static_cast<const CudaError*>(exc)->msg; }
+
+}  // namespace taral
+
+// ================================================================================================ C ABI
+using taral::EngineBase;
+
+struct pdhg_ctx {
+    std::unique_ptr<EngineBase> e;
+    int precision = TARAL_FP64;
+    bool started = false;
+    std::string err;
+};
+
+static int fail(pdhg_ctx* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    return code;
+}
+
+#define GUARD(ctx, body)                                                             \
+    try {                                                                            \
+        body;                                                                        \
+        return TARAL_OK;                                                             \
+    } catch (const taral::CudaError& ex) {                                           \
+        return fail(ctx, TARAL_ERR_CUDA, ex.msg);                                    \
+    } catch (const std::bad_alloc&) {                                                \
+        return fail(ctx, TARAL_ERR_ALLOC, "host allocation failed");                 \
+    } catch (const std::exception& ex) {                                             \
+        return fail(ctx, TARAL_ERR_INPUT, ex.what());                                \
+    }
+
+static std::string check_csr(const taral_csr* a, int rows, int cols, const char* name) {
+    if (!a) return std::string(name) + " is NULL";
+    if (a->rows != rows || a->cols != cols) return std::string(name) + " has the wrong shape";
+    if (a->nnz < 0 || a->nnz > INT32_MAX - 64) return std::string(name) + ": nnz out of the int32 range";
+    if (!a->ptr || (a->nnz && (!a->idx || !a->val))) return std::string(name) + ": NULL array";
+    if (a->ptr[0] != 0 || a->ptr[rows] != a->nnz) return std::string(name) + ": ptr does not span [0, nnz]";
+    for (int r = 0; r < rows; ++r)
+        if (a->ptr[r + 1] < a->ptr[r]) return std::string(name) + ": ptr is not monotone";
+    for (int64_t k = 0; k < a->nnz; ++k)
+        if (a->idx[k] < 0 || a->idx[k] >= cols) return std::string(name) + ": column index out of range";
+    return "";
+}
+
+extern "C" int pdhg_create(const taral_csr* A, const taral_csr* AT, const double* c, const double* l,
+                           const double* u, const double* rl, const double* ru, const double* Dr, const double* Dc,
+                           int m, int n, int precision, int eval_freq, unsigned flags, pdhg_ctx** out) {
+    if (!out) return TARAL_ERR_INPUT;
+    *out = nullptr;
+    if (m < 0 || n < 0) return TARAL_ERR_INPUT;
+    if (precision != TARAL_FP64 && precision != TARAL_FP32) return TARAL_ERR_INPUT;
+    if (!check_csr(A, m, n, "A").empty() || !check_csr(AT, n, m, "AT").empty() || A->nnz != AT->nnz)
+        return TARAL_ERR_INPUT;
+    if ((n && (!c || !l || !u || !Dc)) || (m && (!rl || !ru || !Dr))) return TARAL_ERR_INPUT;
+    int dev_count = 0;
+    if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0) return TARAL_ERR_NO_DEVICE;
+    auto* ctx = new pdhg_ctx;
+    ctx->precision = precision;
+    try {
+        ctx->e = taral::make_engine(precision);
+        taral::engine_init(*ctx->e, precision, *A, *AT, c, l, u, rl, ru, Dr, Dc, m, n, eval_freq, flags);
+    } catch (const taral::CudaError& ex) {
+        std::string msg = ex.msg;
+        delete ctx;
+        return msg.find("cudaMalloc") != std::string::npos ? TARAL_ERR_ALLOC : TARAL_ERR_CUDA;
+    } catch (const std::bad_alloc&) {
+        delete ctx;
+        return TARAL_ERR_ALLOC;
+    }
+    *out = ctx;
+    return TARAL_OK;
+}
+
+extern "C" int pdhg_power_norm(pdhg_ctx* ctx, int iters, double* norm_out) {
+    if (!ctx || !norm_out) return TARAL_ERR_INPUT;
+    GUARD(ctx, *norm_out = ctx->e->power_norm(iters))
+}
+extern "C" int pdhg_set_steps(pdhg_ctx* ctx, double tau, double sigma) {
+    if (!ctx) return TARAL_ERR_INPUT;
+    GUARD(ctx, ctx->e->set_steps(tau, sigma))
+}
+extern "C" int pdhg_start(pdhg_ctx* ctx, const double* x0, const double* z0) {
+    if (!ctx) return TARAL_ERR_INPUT;
+    GUARD(ctx, ctx->e->start(x0, z0); ctx->started = true)
+}
+extern "C" int pdhg_iterate(pdhg_ctx* ctx, int steps) {
+    if (!ctx || steps < 0) return TARAL_ERR_INPUT;
+    if (!ctx->started) return fail(ctx, TARAL_ERR_STATE, "pdhg_iterate before pdhg_start");
+    GUARD(ctx, ctx->e->iterate(steps))
+}
+extern "C" int pdhg_eval(pdhg_ctx* ctx, int avg, double f, double out[10]) {
+    if (!ctx || !out) return TARAL_ERR_INPUT;
+    if (!ctx->started) return fail(ctx, TARAL_ERR_STATE, "pdhg_eval before pdhg_start");
+    GUARD(ctx, ctx->e->eval(avg != 0, f, out))
+}
+extern "C" int pdhg_eval_pair(pdhg_ctx* ctx, double f, double cur[10], double avg[10]) {
+    if (!ctx || !cur || !avg) return TARAL_ERR_INPUT;
+    if (!ctx->started) return fail(ctx, TARAL_ERR_STATE, "pdhg_eval_pair before pdhg_start");
+    GUARD(ctx, ctx->e->eval_pair(f, cur, avg))
+}
+extern "C" int pdhg_restart(pdhg_ctx* ctx, int avg, double f) {
+    if (!ctx) return TARAL_ERR_INPUT;
+    if (!ctx->started) return fail(ctx, TARAL_ERR_STATE, "pdhg_restart before pdhg_start");
+    GUARD(ctx, ctx->e->restart(avg != 0, f))
+}
+extern "C" int pdhg_download(pdhg_ctx* ctx, int avg, double f, double* x, double* z) {
+    if (!ctx || !x || !z) return TARAL_ERR_INPUT;
+    GUARD(ctx, ctx->e->download(avg != 0, f, x, z))
+}
+extern "C" int pdhg_info(pdhg_ctx* ctx, char* name_out, size_t cap, size_t* mem_used) {
+    if (!ctx) return TARAL_ERR_INPUT;
+    if (name_out && cap) {
+        std::snprintf(name_out, cap, "%s", ctx->e->name.c_str());
+    }
+    if (mem_used) *mem_used = ctx->e->mem_used;
+    return TARAL_OK;
+}
+extern "C" int64_t pdhg_kernel_launches(const pdhg_ctx* ctx) { return ctx ? ctx->e->launches : 0; }
+extern "C" const char* pdhg_last_error(const pdhg_ctx* ctx) { return ctx ? ctx->err.c_str() : "NULL context"; }
+extern "C" void pdhg_destroy(pdhg_ctx* ctx) { delete ctx; }
+
+// ================================================================================================ SpMV plan
+struct taral_spmv_plan {
+    int rows = 0, cols = 0, dtype = TARAL_FP64, nblk = 0;
+    int* blk = nullptr;
+};
+
+extern "C" int taral_spmv_plan_create(int rows, int cols, const int64_t* host_ptr, int dtype, taral_spmv_plan** out) {
+    if (!out || rows < 0 || cols < 0 || !host_ptr) return TARAL_ERR_INPUT;
+    if (dtype != TARAL_FP64 && dtype != TARAL_FP32) return TARAL_ERR_INPUT;
+    *out = nullptr;
+    for (int r = 0; r < rows; ++r)
+        if (host_ptr[r + 1] < host_ptr[r]) return TARAL_ERR_INPUT;
+    if (host_ptr[rows] > INT32_MAX - 64) return TARAL_ERR_INPUT;
+    std::vector<int> blk = taral::build_row_blocks(host_ptr, rows);
+    auto* p = new taral_spmv_plan;
+    p->rows = rows, p->cols = cols, p->dtype = dtype, p->nblk = int(blk.size()) - 1;
+    if (cudaMalloc(&p->blk, blk.size() * sizeof(int)) != cudaSuccess) {
+        delete p;
+        return TARAL_ERR_ALLOC;
+    }
+    if (cudaMemcpy(p->blk, blk.data(), blk.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaFree(p->blk);
+        delete p;
+        return TARAL_ERR_CUDA;
+    }
+    *out = p;
+    return TARAL_OK;
+}
+
+template <class T>
+static void spmv_launch(const taral_spmv_plan* p, const int* ptr, const int* idx, const void* val, const void* x,
+                        void* y, cudaStream_t s) {
+    using namespace taral;
+    bool vec = (reinterpret_cast<uintptr_t>(idx) % 16 == 0) && (reinterpret_cast<uintptr_t>(val) % 16 == 0);
+    EpiStore<T> e{static_cast<T*>(y)};
+    if (vec)
+        k_rowblock<T, T, EpiStore<T>, true><<<p->nblk, kThreads, 0, s>>>(ptr, idx, static_cast<const T*>(val),
+                                                                          static_cast<const T*>(x), p->blk, nullptr, e);
+    else
+        k_rowblock<T, T, EpiStore<T>, false><<<p->nblk, kThreads, 0, s>>>(ptr, idx, static_cast<const T*>(val),
+                                                                           static_cast<const T*>(x), p->blk, nullptr, e);
+}
+
+extern "C" int taral_spmv_run(const taral_spmv_plan* p, const int32_t* d_ptr, const int32_t* d_idx, const void* d_val,
+                              const void* d_x, void* d_y, void* stream) {
+    if (!p || !d_ptr || !d_x || !d_y) return TARAL_ERR_INPUT;
+    if (p->nblk == 0) return TARAL_OK;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (p->dtype == TARAL_FP32) spmv_launch<float>(p, d_ptr, d_idx, d_val, d_x, d_y, s);
+    else spmv_launch<double>(p, d_ptr, d_idx, d_val, d_x, d_y, s);
+    return cudaGetLastError() == cudaSuccess ? TARAL_OK : TARAL_ERR_CUDA;
+}
+extern "C" int taral_spmv_plan_blocks(const taral_spmv_plan* p) { return p ? p->nblk : 0; }
+extern "C" void taral_spmv_plan_destroy(taral_spmv_plan* p) {
+    if (!p) return;
+    cudaFree(p->blk);
+    delete p;
+}

@@ -1,0 +1,35 @@
+// Internal interface between the C ABI / host driver and the device engine (one object per context).
+#pragma once
+#include <cstdint>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/taral_pdhg.h"
+
+namespace taral {
+
+// The backend concept of the reference driver (gpu/pdhg.cu:761-849 calls these on Gpu<T> / Cpu<T>).
+struct EngineBase {
+    std::string name;
+    size_t mem_used = 0;
+    int64_t launches = 0;
+    virtual ~EngineBase() = default;
+    virtual double power_norm(int iters) = 0;
+    virtual void set_steps(double tau, double sigma) = 0;
+    virtual void start(const double* x0, const double* z0) = 0;
+    virtual void iterate(int steps) = 0;
+    virtual void eval(bool avg, double f, double* out10) = 0;
+    virtual void eval_pair(double f, double* cur10, double* avg10) = 0;
+    virtual void restart(bool avg, double f) = 0;
+    virtual void download(bool avg, double f, double* x, double* z) = 0;
+    virtual void sync() = 0;
+};
+
+std::unique_ptr<EngineBase> make_engine(int precision);
+void engine_init(EngineBase& e, int precision, const taral_csr& A, const taral_csr& AT, const double* c,
+                 const double* l, const double* u, const double* rl, const double* ru, const double* Dr,
+                 const double* Dc, int m, int n, int eval_freq, unsigned flags);
+std::vector<int> build_row_blocks(const int64_t* ptr, int rows);
+
+}  // namespace taral

@@ -1,0 +1,347 @@
+// MPS reader with the semantics of the reference reader (src/mps.cpp:1-399): whitespace-separated fields first,
+// fixed columns as the fallback; OBJSENSE, RANGES, the usual bound types, integer MARKER blocks and quadratic
+// objective sections; only the first named RHS / RANGES / BOUNDS set is used. Malformed input is an error:
+// missing ENDATA, a repeated ROWS or COLUMNS section, duplicate row names, a column in two separate blocks,
+// names used before they are declared and numbers outside the plain decimal grammar (hex, inf, nan, overflow).
+// Entries of one column are sorted by row, duplicates summed in file order and zero sums dropped.
+#include <algorithm>
+#include <cctype>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <sstream>
+#include <unordered_map>
+#include <unordered_set>
+
+#include "host.hpp"
+
+namespace taral {
+namespace {
+
+constexpr double kHuge = 1e20;  // |bound| >= 1e20 is infinite
+
+double parse_number(const std::string& s) {
+    size_t i = 0, n = s.size();
+    auto digits = [&] {
+        size_t a = i;
+        while (i < n && std::isdigit(static_cast<unsigned char>(s[i]))) ++i;
+        return i - a;
+    };
+    if (i < n && (s[i] == '+' || s[i] == '-')) ++i;
+    size_t mant = digits();
+    if (i < n && s[i] == '.') ++i, mant += digits();
+    bool ok = mant > 0;
+    if (ok && i < n && std::strchr("eEdD", s[i])) {
+        ++i;
+        if (i < n && (s[i] == '+' || s[i] == '-')) ++i;
+        ok = digits() > 0;
+    }
+    if (!ok || i != n) throw ParseError("bad number '" + s + "'");
+    std::string t = s;
+    for (char& ch : t)
+        if (ch == 'd' || ch == 'D') ch = 'E';
+    double v = std::strtod(t.c_str(), nullptr);
+    if (!std::isfinite(v)) throw ParseError("number '" + s + "' is not finite");
+    return v;
+}
+
+std::string fixed_field(const std::string& line, size_t a, size_t b) {
+    if (line.size() <= a) return "";
+    std::string s = line.substr(a, b - a);
+    size_t i = s.find_first_not_of(" \t"), j = s.find_last_not_of(" \t\r");
+    return i == std::string::npos ? "" : s.substr(i, j - i + 1);
+}
+
+std::vector<std::string> split(const std::string& line, const std::string& section, bool fixed) {
+    std::vector<std::string> t;
+    if (!fixed) {
+        auto ws = [](char c) { return c == ' ' || c == '\t' || c == '\n' || c == '\v' || c == '\f' || c == '\r'; };
+        size_t p = 0, e = line.size();
+        while (p < e) {
+            while (p < e && ws(line[p])) ++p;
+            size_t s = p;
+            while (p < e && !ws(line[p])) ++p;
+            if (p > s) t.emplace_back(line, s, p - s);
+        }
+        return t;
+    }
+    auto f = [&](size_t a, size_t b) { t.push_back(fixed_field(line, a, b)); };
+    if (section == "ROWS") {
+        f(1, 3), f(4, 12);
+    } else if (section == "BOUNDS") {
+        f(1, 3), f(4, 12), f(14, 22);
+        if (!fixed_field(line, 24, 36).empty()) f(24, 36);
+    } else {
+        f(4, 12), f(14, 22), f(24, 36);
+        if (!fixed_field(line, 39, 47).empty()) f(39, 47), f(49, 61);
+    }
+    return t;
+}
+
+struct Entry {
+    int32_t row;
+    double v;
+};
+
+Model parse(const std::string& path, bool fixed) {
+    std::ifstream in(path);
+    if (!in) throw ParseError("cannot open " + path);
+    Model md;
+    std::string section, obj_row, line;
+    std::unordered_map<std::string, int> row_id, col_id;
+    std::unordered_set<std::string> free_rows, seen;
+    std::vector<char> row_type;
+    std::vector<double> rhs, range;
+    std::vector<char> has_range;
+    bool in_int = false, endata = false, q_full = false;
+    int cur = -1;
+    std::vector<Entry> pending;
+    std::string rhs_set, range_set, bound_set;
+    std::map<std::pair<int, int>, double> q;
+
+    auto close_column = [&] {  // sorted by row, duplicates summed in file order, zero sums dropped
+        if (cur < 0) return;
+        std::stable_sort(pending.begin(), pending.end(), [](const Entry& a, const Entry& b) { return a.row < b.row; });
+        size_t start = md.row_idx.size();
+        for (const Entry& e : pending) {
+            if (md.row_idx.size() > start && md.row_idx.back() == e.row) md.val.back() += e.v;
+            else md.row_idx.push_back(e.row), md.val.push_back(e.v);
+        }
+        size_t w = start;
+        for (size_t k = start; k < md.row_idx.size(); ++k)
+            if (md.val[k] != 0) md.row_idx[w] = md.row_idx[k], md.val[w] = md.val[k], ++w;
+        md.row_idx.resize(w), md.val.resize(w);
+        md.col_ptr.push_back(int64_t(w));
+        pending.clear();
+    };
+    auto first_set = [](std::string& keep, const std::string& nm) {
+        if (keep.empty()) keep = nm;
+        return keep == nm;
+    };
+    auto row_of = [&](const std::string& nm) -> int {
+        auto it = row_id.find(nm);
+        if (it != row_id.end()) return it->second;
+        if (nm == obj_row) return -1;
+        if (free_rows.count(nm)) return -2;
+        throw ParseError("unknown row '" + nm + "'");
+    };
+    auto col_of = [&](const std::string& nm) {
+        auto it = col_id.find(nm);
+        if (it == col_id.end()) throw ParseError("unknown column '" + nm + "'");
+        return it->second;
+    };
+
+    while (std::getline(in, line)) {
+        if (!line.empty() && line.back() == '\r') line.pop_back();
+        if (line.find_first_not_of(" \t") == std::string::npos || line[0] == '*') continue;
+        if (line[0] != ' ' && line[0] != '\t') {  // section header
+            std::istringstream hs(line);
+            std::string arg;
+            hs >> section >> arg;
+            if (section == "NAME") {
+                md.name = arg;
+            } else if (section == "ENDATA") {
+                endata = true;
+                break;
+            } else if (section == "OBJSENSE") {
+                if (!arg.empty()) {
+                    if (arg == "MAX" || arg == "MAXIMIZE") md.maximize = true;
+                    else if (arg != "MIN" && arg != "MINIMIZE") throw ParseError("bad OBJSENSE " + arg);
+                }
+            } else if (section == "QUADOBJ" || section == "QMATRIX") {
+                q_full = section == "QMATRIX";
+                section = "QUAD";
+            } else if (section == "QSECTION" || section == "QCMATRIX") {
+                if (section == "QCMATRIX" || arg != obj_row)
+                    throw ParseError("quadratic constraints are not supported (" + section + " " + arg + ")");
+                q_full = true;
+                section = "QUAD";
+            } else if (section != "ROWS" && section != "COLUMNS" && section != "RHS" && section != "RANGES" &&
+                       section != "BOUNDS") {
+                throw ParseError("unsupported section " + section);
+            }
+            if ((section == "ROWS" || section == "COLUMNS") && !seen.insert(section).second)
+                throw ParseError("section " + section + " appears twice");
+            continue;
+        }
+        std::vector<std::string> t = split(line, section, fixed);
+        if (section == "OBJSENSE") {
+            std::string v = t.empty() ? "" : t[0];
+            if (v == "MAX" || v == "MAXIMIZE") md.maximize = true;
+            else if (v != "MIN" && v != "MINIMIZE") throw ParseError("bad OBJSENSE " + v);
+        } else if (section == "ROWS") {
+            if (t.size() != 2 || t[1].empty()) throw ParseError("bad ROWS line");
+            char type = t[0].empty() ? '?' : char(std::toupper(static_cast<unsigned char>(t[0][0])));
+            if (row_id.count(t[1]) || t[1] == obj_row || free_rows.count(t[1]))
+                throw ParseError("duplicate row name '" + t[1] + "'");
+            if (type == 'N') {
+                if (obj_row.empty()) obj_row = t[1];
+                else free_rows.insert(t[1]);
+            } else if (type == 'E' || type == 'L' || type == 'G') {
+                row_id[t[1]] = int(md.row_names.size());
+                md.row_names.push_back(t[1]);
+                row_type.push_back(type);
+            } else {
+                throw ParseError("bad row type " + t[0]);
+            }
+        } else if (section == "COLUMNS") {
+            if (t.size() >= 2 && t[1] == "'MARKER'") {
+                bool s = false, e = false;
+                for (const std::string& w : t) s |= w == "'INTORG'", e |= w == "'INTEND'";
+                if (s == e) throw ParseError("bad MARKER line");
+                in_int = s;
+                continue;
+            }
+            if (t.size() != 3 && t.size() != 5) throw ParseError("bad COLUMNS line");
+            int j;
+            if (cur >= 0 && t[0] == md.col_names[cur]) {
+                j = cur;
+            } else {
+                auto it = col_id.find(t[0]);
+                if (it != col_id.end()) throw ParseError("column '" + t[0] + "' is listed in two separate blocks");
+                close_column();
+                j = int(md.col_names.size());
+                col_id[t[0]] = j;
+                md.col_names.push_back(t[0]);
+                md.cost.push_back(0);
+                md.is_int.push_back(in_int ? 1 : 0);
+            }
+            cur = j;
+            for (size_t k = 1; k + 1 < t.size(); k += 2) {
+                int r = row_of(t[k]);
+                double v = parse_number(t[k + 1]);
+                if (r == -1) md.cost[j] += v;
+                else if (r >= 0) pending.push_back({r, v});
+            }
+        } else if (section == "RHS" || section == "RANGES") {
+            size_t start = fixed ? 1 : (t.size() % 2 == 1 ? 1 : 0);
+            if (start == 1 && !t[0].empty() && !first_set(section == "RHS" ? rhs_set : range_set, t[0])) continue;
+            if (rhs.empty()) {
+                rhs.assign(md.row_names.size(), 0);
+                range.assign(md.row_names.size(), 0);
+                has_range.assign(md.row_names.size(), 0);
+            }
+            for (size_t k = start; k + 1 < t.size(); k += 2) {
+                int r = row_of(t[k]);
+                double v = parse_number(t[k + 1]);
+                if (section == "RHS") {
+                    if (r == -1) md.obj_const = -v;
+                    else if (r >= 0) rhs[r] = v;
+                } else if (r >= 0) {
+                    range[r] = v, has_range[r] = 1;
+                }
+            }
+        } else if (section == "BOUNDS") {
+            if (md.col_lo.empty()) {
+                md.col_lo.assign(md.col_names.size(), 0);
+                md.col_up.assign(md.col_names.size(), kInf);
+            }
+            std::string type = t.empty() ? "" : t[0];
+            bool no_value = type == "FR" || type == "MI" || type == "PL" || type == "BV";
+            std::string set, col, val;
+            if (fixed) {
+                set = t.size() > 1 ? t[1] : "", col = t.size() > 2 ? t[2] : "", val = t.size() > 3 ? t[3] : "";
+            } else if (t.size() == 4) {
+                set = t[1], col = t[2], val = t[3];
+            } else if (t.size() == 3) {
+                if (no_value) set = t[1], col = t[2];
+                else col = t[1], val = t[2];
+            } else if (t.size() == 2) {
+                col = t[1];
+            } else {
+                throw ParseError("bad BOUNDS line");
+            }
+            if (!set.empty() && !first_set(bound_set, set)) continue;
+            auto it = col_id.find(col);
+            if (it == col_id.end()) throw ParseError("unknown column '" + col + "' in BOUNDS");
+            int j = it->second;
+            double v = no_value || val.empty() ? 0 : parse_number(val);
+            double &lo = md.col_lo[j], &up = md.col_up[j];
+            if (type == "BV" || type == "LI" || type == "UI") md.is_int[j] = 1;
+            if (type == "LO" || type == "LI") lo = v;
+            else if (type == "UP" || type == "UI") {
+                up = v;
+                if (v < 0 && lo == 0) lo = -kInf;
+            } else if (type == "FX") lo = up = v;
+            else if (type == "FR") lo = -kInf, up = kInf;
+            else if (type == "MI") lo = -kInf;
+            else if (type == "PL") up = kInf;
+            else if (type == "BV") lo = 0, up = 1;
+            else throw ParseError("unsupported bound type " + type);
+        } else if (section == "QUAD") {
+            if (t.size() != 3) throw ParseError("bad quadratic objective line");
+            int a = col_of(t[0]), b = col_of(t[1]);
+            double v = parse_number(t[2]);
+            if (q_full && a < b) continue;
+            q[{std::max(a, b), std::min(a, b)}] += v;
+        }
+    }
+    close_column();
+    if (!endata) throw ParseError("missing ENDATA");
+    for (const auto& kv : q)
+        if (kv.second != 0) ++md.n_quadratic;
+    if (obj_row.empty()) throw ParseError("no objective row");
+
+    size_t m = md.row_names.size(), n = md.col_names.size();
+    if (md.col_ptr.size() != n + 1) throw ParseError("internal: column pointer size");
+    if (rhs.empty()) rhs.assign(m, 0), range.assign(m, 0), has_range.assign(m, 0);
+    if (md.col_lo.empty()) md.col_lo.assign(n, 0), md.col_up.assign(n, kInf);
+    md.row_lo.resize(m), md.row_up.resize(m);
+    for (size_t i = 0; i < m; ++i) {
+        double b = rhs[i], R = range[i];
+        double &lo = md.row_lo[i], &up = md.row_up[i];
+        if (row_type[i] == 'E') {
+            lo = up = b;
+            if (has_range[i]) (R >= 0 ? up : lo) = b + R;
+        } else if (row_type[i] == 'L') {
+            up = b;
+            lo = has_range[i] ? b - std::fabs(R) : -kInf;
+        } else {
+            lo = b;
+            up = has_range[i] ? b + std::fabs(R) : kInf;
+        }
+    }
+    for (std::vector<double>* lo : {&md.col_lo, &md.row_lo})
+        for (double& v : *lo)
+            if (v <= -kHuge) {
+                if (std::isfinite(v)) ++md.sentinel_bounds;
+                v = -kInf;
+            }
+    for (std::vector<double>* up : {&md.col_up, &md.row_up})
+        for (double& v : *up)
+            if (v >= kHuge) {
+                if (std::isfinite(v)) ++md.sentinel_bounds;
+                v = kInf;
+            }
+    return md;
+}
+
+}  // namespace
+
+Model read_mps(const std::string& path) {
+    try {
+        return parse(path, false);
+    } catch (const ParseError& free_err) {
+        try {
+            return parse(path, true);
+        } catch (const ParseError& fixed_err) {
+            if (std::string(free_err.what()) == fixed_err.what()) throw;
+            throw ParseError(std::string(free_err.what()) + " (free format); " + fixed_err.what() + " (fixed columns)");
+        }
+    }
+}
+
+taral_model Model::view() const {
+    taral_model v{};
+    v.m = int(row_lo.size()), v.n = int(cost.size());
+    v.col_ptr = col_ptr.data(), v.row_idx = row_idx.data(), v.val = val.data();
+    v.cost = cost.data(), v.col_lo = col_lo.data(), v.col_up = col_up.data();
+    v.row_lo = row_lo.data(), v.row_up = row_up.data();
+    v.obj_const = obj_const, v.maximize = maximize ? 1 : 0;
+    v.is_int = is_int.data(), v.n_quadratic = n_quadratic;
+    return v;
+}
+
+}  // namespace taral

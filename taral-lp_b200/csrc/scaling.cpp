@@ -1,0 +1,122 @@
+// Host preprocessing: CSR transpose and Ruiz / Pock-Chambolle scaling (gpu/pdhg.cu:55-133 semantics).
+// FP64, single pass order identical to the reference so the scaled matrix is bit-identical to it.
+#include <algorithm>
+#include <cmath>
+
+#include "host.hpp"
+
+namespace taral {
+
+Csr transpose(const Csr& a, int cols) {  // counting sort; rows of the output ascending (gpu/pdhg.cu:55-70)
+    Csr t;
+    t.rows = cols;
+    t.ptr.assign(size_t(cols) + 1, 0);
+    for (int32_t k : a.idx) t.ptr[size_t(k) + 1]++;
+    for (int j = 0; j < cols; ++j) t.ptr[j + 1] += t.ptr[j];
+    t.idx.resize(a.idx.size());
+    t.val.resize(a.val.size());
+    std::vector<int64_t> pos(t.ptr.begin(), t.ptr.end() - 1);
+    for (int i = 0; i < a.rows; ++i)
+        for (int64_t k = a.ptr[i]; k < a.ptr[i + 1]; ++k) {
+            int64_t p = pos[a.idx[k]]++;
+            t.idx[p] = i, t.val[p] = a.val[k];
+        }
+    return t;
+}
+
+Scaled build_scaled(const taral_model& md, double sign) {
+    Scaled P;
+    P.n = md.n, P.m = md.m;
+    Csr T;  // A^T from the column-wise model, zero entries dropped
+    T.rows = P.n;
+    T.ptr.assign(size_t(P.n) + 1, 0);
+    const int64_t base = md.col_ptr[0];
+    T.idx.reserve(size_t(md.col_ptr[P.n] - base));
+    T.val.reserve(size_t(md.col_ptr[P.n] - base));
+    for (int j = 0; j < P.n; ++j) {
+        for (int64_t k = md.col_ptr[j]; k < md.col_ptr[j + 1]; ++k)
+            if (md.val[k] != 0) T.idx.push_back(md.row_idx[k]), T.val.push_back(md.val[k]);
+        T.ptr[j + 1] = int64_t(T.idx.size());
+    }
+    P.A = transpose(T, P.m);
+    T = Csr();
+    Csr& A = P.A;
+    P.Dr.assign(size_t(P.m), 1), P.Dc.assign(size_t(P.n), 1);
+    std::vector<double> rs(size_t(P.m)), cs(size_t(P.n));
+    auto apply = [&] {  // divide by sqrt of the row and column measures, fold the factors into Dr, Dc
+        for (double& v : rs) v = v > 0 ? std::sqrt(v) : 1;
+        for (double& v : cs) v = v > 0 ? std::sqrt(v) : 1;
+        for (int i = 0; i < P.m; ++i) {
+            const double ri = rs[i];
+            for (int64_t k = A.ptr[i]; k < A.ptr[i + 1]; ++k) A.val[k] /= ri * cs[A.idx[k]];
+        }
+        for (int i = 0; i < P.m; ++i) P.Dr[i] /= rs[i];
+        for (int j = 0; j < P.n; ++j) P.Dc[j] /= cs[j];
+    };
+    for (int pass = 0; pass < 10; ++pass) {  // Ruiz equilibration, inf-norm
+        std::fill(rs.begin(), rs.end(), 0.0), std::fill(cs.begin(), cs.end(), 0.0);
+        for (int i = 0; i < P.m; ++i) {
+            double ri = 0;
+            for (int64_t k = A.ptr[i]; k < A.ptr[i + 1]; ++k) {
+                double a = std::fabs(A.val[k]);
+                ri = std::max(ri, a);
+                double& cj = cs[A.idx[k]];
+                cj = std::max(cj, a);
+            }
+            rs[i] = ri;
+        }
+        apply();
+    }
+    std::fill(rs.begin(), rs.end(), 0.0), std::fill(cs.begin(), cs.end(), 0.0);  // Pock-Chambolle, alpha = 1
+    for (int i = 0; i < P.m; ++i)
+        for (int64_t k = A.ptr[i]; k < A.ptr[i + 1]; ++k) rs[i] += std::fabs(A.val[k]), cs[A.idx[k]] += std::fabs(A.val[k]);
+    apply();
+    P.AT = transpose(A, P.n);
+    P.c.resize(size_t(P.n)), P.l.resize(size_t(P.n)), P.u.resize(size_t(P.n));
+    P.rl.resize(size_t(P.m)), P.ru.resize(size_t(P.m));
+    for (int j = 0; j < P.n; ++j) {
+        double c = sign * md.cost[j];
+        P.cnorm += c * c;
+        P.c[j] = c * P.Dc[j], P.l[j] = md.col_lo[j] / P.Dc[j], P.u[j] = md.col_up[j] / P.Dc[j];
+    }
+    for (int i = 0; i < P.m; ++i) {
+        double lo = md.row_lo[i], up = md.row_up[i], b = 0;
+        if (std::isfinite(lo) && std::isfinite(up)) b = std::max(std::fabs(lo), std::fabs(up));
+        else if (std::isfinite(lo)) b = std::fabs(lo);
+        else if (std::isfinite(up)) b = std::fabs(up);
+        P.bnorm += b * b;
+        P.rl[i] = lo * P.Dr[i], P.ru[i] = up * P.Dr[i];
+    }
+    P.bnorm = std::sqrt(P.bnorm), P.cnorm = std::sqrt(P.cnorm);
+    return P;
+}
+
+Finished finish_point(const taral_model& md, const Scaled& P, const Outcome& r) {
+    Finished f;
+    f.x.resize(size_t(P.n));
+    f.y.resize(size_t(P.m));
+    for (int j = 0; j < P.n; ++j) f.x[j] = r.x[j] * P.Dc[j];
+    for (int i = 0; i < P.m; ++i) f.y[i] = P.Dr[i] * r.z[i];
+    long double obj = md.obj_const;
+    for (int j = 0; j < P.n; ++j) obj += (long double)md.cost[j] * f.x[j];
+    std::vector<double> ax(size_t(P.m), 0.0);
+    double bviol = 0, rviol = 0;
+    for (int j = 0; j < P.n; ++j) {
+        for (int64_t k = md.col_ptr[j]; k < md.col_ptr[j + 1]; ++k) ax[md.row_idx[k]] += md.val[k] * f.x[j];
+        bviol = std::max(bviol, std::max(md.col_lo[j] - f.x[j], f.x[j] - md.col_up[j]));
+    }
+    for (int i = 0; i < P.m; ++i) rviol = std::max(rviol, std::max(md.row_lo[i] - ax[i], ax[i] - md.row_up[i]));
+    f.objective = double(obj), f.max_row_violation = rviol, f.max_bound_violation = bviol;
+    return f;
+}
+
+const char* status_name(int s) {
+    switch (s) {
+        case TARAL_NEAR_OPTIMAL: return "near_optimal";
+        case TARAL_TIME_LIMIT: return "time_limit";
+        case TARAL_NUMERICAL_FAILURE: return "numerical_failure";
+        default: return "iteration_limit";
+    }
+}
+
+}  // namespace taral

@@ -282,7 +282,7 @@ def planted(m: int, n: int, per_col: int = 5, seed: int = 0, zipf: Optional[floa
         rows = np.sort(slots.reshape(n, per_col), axis=1)
         keep = np.ones(rows.shape, bool)
         keep[:, 1:] = rows[:, 1:] != rows[:, :-1]
-    vals = rng.standard_normal(rows.shape)
+    vals = _r12(rng.standard_normal(rows.shape))
     col_ptr, ri, v = _csc_from_lists(n, rows, vals, keep=keep)
     u = rng.random(n)
     x = np.where(u < 0.4, 0.0, np.where(u < 0.5, 10.0, 0.0))
@@ -296,8 +296,48 @@ def planted(m: int, n: int, per_col: int = 5, seed: int = 0, zipf: Optional[floa
     np.add.at(b, ri, v * x[cols])
     aty = np.zeros(n)
     np.add.at(aty, cols, v * y[ri])
-    c = aty + z
+    b, c = _r12(b), _r12(aty + z)  # every number as the MPS file carries it; x*, y* stay optimal to ~1e-12
     obj = float(np.dot(c, x))
     return LP(name=name or f"PLANTED_{m}x{n}", m=m, n=n, col_ptr=col_ptr, row_idx=ri, val=v, cost=c,
               col_lo=np.zeros(n), col_up=np.full(n, 10.0), row_lo=b.copy(), row_up=b.copy(),
               row_types=["E"] * m, x_star=x, y_star=y, obj_star=obj)
+
+
+# ---------------------------------------------------------------------------------------------- general LP
+def general(m: int, n: int, per_col: int = 4, seed: int = 0, maximize: bool = False) -> LP:
+    """Bounded LP with every row and bound kind: E, L, G and ranged rows; free, lower-only, upper-only, boxed
+    and fixed columns. A planted primal point x0 is feasible (rows hold A x0 with slack on their open side) and
+    planted multipliers y0 / reduced costs d make the dual feasible (sign of y by row kind, sign of d by which
+    column bounds are finite), so the optimum is finite. Values N(0,1) rounded to 6 decimals."""
+    rng = np.random.default_rng(seed)
+    rows = _distinct_rows(rng, m, n, per_col)
+    vals = np.round(rng.standard_normal(rows.shape), 6)
+    vals[vals == 0] = 0.5
+    col_ptr, ri, v = _csc_from_lists(n, rows, vals)
+    ck = rng.choice(5, n, p=[0.1, 0.3, 0.1, 0.4, 0.1])  # 0 free, 1 lower, 2 upper, 3 boxed, 4 fixed
+    x0 = np.round(rng.uniform(-2, 2, n), 3)
+    lo = np.where(np.isin(ck, (1, 3)), x0 - np.round(rng.uniform(0, 2, n), 3), -INF)
+    up = np.where(np.isin(ck, (2, 3)), x0 + np.round(rng.uniform(0, 2, n), 3), INF)
+    lo = _r12(np.where(ck == 4, x0, lo))
+    up = _r12(np.where(ck == 4, x0, up))
+    cols = np.repeat(np.arange(n), np.diff(col_ptr))
+    ax0 = np.zeros(m)
+    np.add.at(ax0, ri, v * x0[cols])
+    rk = rng.choice(4, m, p=[0.3, 0.3, 0.3, 0.1])  # 0 E, 1 L, 2 G, 3 ranged
+    slack = np.round(rng.uniform(0, 1, m), 3)
+    rlo = np.where(rk == 0, ax0, np.where(rk == 2, ax0 - slack, np.where(rk == 3, ax0 - slack, -INF)))
+    rup = np.where(rk == 0, ax0, np.where(rk == 1, ax0 + slack, np.where(rk == 3, ax0 + 1 + slack, INF)))
+    rlo, rup = _r12(rlo), _r12(rup)
+    rup = np.where(rk == 3, rlo + _r12(1 + slack), rup)  # a ranged row is read back as lo + |R|
+    y0 = np.round(rng.standard_normal(m), 3)
+    y0 = np.where(rk == 1, -np.abs(y0), np.where(rk == 2, np.abs(y0), y0))  # min form: y <= 0 on L, >= 0 on G
+    d = np.round(rng.uniform(0, 1, n), 3)
+    d = np.where(ck == 0, 0.0, np.where(ck == 2, -d, np.where(ck == 3, rng.choice([-1, 1], n) * d, d)))
+    aty = np.zeros(n)
+    np.add.at(aty, cols, v * y0[ri])
+    c = _r12(aty + d)
+    types = ["E" if k == 0 else ("L" if k == 1 else "G") for k in rk]
+    if maximize:
+        c = -c
+    return LP(name=f"GENERAL_{m}x{n}_{seed}", m=m, n=n, col_ptr=col_ptr, row_idx=ri, val=v, cost=c,
+              col_lo=lo, col_up=up, row_lo=rlo, row_up=rup, obj_const=0.5, maximize=maximize, row_types=types)

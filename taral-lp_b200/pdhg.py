@@ -1,0 +1,345 @@
+"""Python binding of the engine's C ABI (include/taral_pdhg.h) over ctypes.
+
+Mirrors the reference's interfaces for the PDHG path: the backend concept of gpu/pdhg.cu:313-514
+(:class:`Engine`: power_norm, set_steps, start, iterate, eval, restart, download), the whole solve
+(:func:`solve`, gpu/pdhg.cu:761-911 behind main), the input gate (:func:`input_error`,
+gpu/pdhg_input.hpp:7-17), the MPS reader (:func:`read_mps`, src/mps.cpp:388) and the standalone CSR SpMV
+(:class:`SpmvPlan`, gpu/csr_matvec.cu:23-32). Everything runs in lib/libtaral_pdhg.so; there is no Python or
+CPU fallback, and loading fails loudly when the library has not been built.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+from typing import Optional
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "lib" / "libtaral_pdhg.so"
+CLI_PATH = PKG / "bin" / "pdhg"
+
+OK, ERR_CUDA, ERR_ALLOC, ERR_INPUT, ERR_UNSUPPORTED, ERR_PARSE, ERR_STATE, ERR_NO_DEVICE = 0, -1, -2, -3, -4, -5, -6, -7
+FP64, FP32 = 0, 1
+STATUS = {0: "near_optimal", 1: "iteration_limit", 2: "time_limit", 3: "numerical_failure"}
+KKT_NAMES = ["PR2S", "PR2O", "PR2R", "DROW", "DZ2", "DR2S", "DR2O", "POBJ", "DCOL", "DX2"]
+ERRORS = {ERR_CUDA: "CUDA error", ERR_ALLOC: "allocation failed", ERR_INPUT: "bad input",
+          ERR_UNSUPPORTED: "unsupported model", ERR_PARSE: "parse error", ERR_STATE: "call out of order",
+          ERR_NO_DEVICE: "no CUDA device"}
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int32)
+_lp = C.POINTER(C.c_int64)
+_ubp = C.POINTER(C.c_ubyte)
+
+
+class TaralError(RuntimeError):
+    def __init__(self, code, msg=""):
+        super().__init__(f"{ERRORS.get(code, code)} ({code}){': ' + msg if msg else ''}")
+        self.code = code
+
+
+class CsrT(C.Structure):
+    _fields_ = [("rows", C.c_int), ("cols", C.c_int), ("nnz", C.c_int64), ("ptr", _lp), ("idx", _ip), ("val", _dp)]
+
+
+class ModelT(C.Structure):
+    _fields_ = [("m", C.c_int), ("n", C.c_int), ("col_ptr", _lp), ("row_idx", _ip), ("val", _dp), ("cost", _dp),
+                ("col_lo", _dp), ("col_up", _dp), ("row_lo", _dp), ("row_up", _dp), ("obj_const", C.c_double),
+                ("maximize", C.c_int), ("is_int", _ubp), ("n_quadratic", C.c_int64)]
+
+
+class OptionsT(C.Structure):
+    _fields_ = [("tol", C.c_double), ("time_limit", C.c_double), ("max_iter", C.c_int64), ("eval_freq", C.c_int),
+                ("row_rel", C.c_double), ("verbose", C.c_int), ("graph", C.c_int), ("precision", C.c_int)]
+
+
+class OutcomeT(C.Structure):
+    _fields_ = [("status", C.c_int), ("iterations", C.c_int64), ("restarts", C.c_int), ("from_average", C.c_int),
+                ("rel_primal", C.c_double), ("rel_dual", C.c_double), ("rel_gap", C.c_double),
+                ("norm_a", C.c_double), ("primal_weight", C.c_double), ("objective", C.c_double),
+                ("max_row_violation", C.c_double), ("max_bound_violation", C.c_double), ("scale_s", C.c_double),
+                ("device_init_s", C.c_double), ("transfer_s", C.c_double), ("solve_s", C.c_double),
+                ("power_iter_s", C.c_double), ("device_mem_bytes", C.c_size_t), ("kernel_launches", C.c_int64),
+                ("nnz", C.c_int64)]
+
+
+# Every symbol the header declares, with its ctypes signature: (restype, argtypes).
+SIGNATURES = {
+    "pdhg_create": (C.c_int, [C.POINTER(CsrT), C.POINTER(CsrT)] + [_dp] * 7 +
+                    [C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint, C.POINTER(C.c_void_p)]),
+    "pdhg_power_norm": (C.c_int, [C.c_void_p, C.c_int, _dp]),
+    "pdhg_set_steps": (C.c_int, [C.c_void_p, C.c_double, C.c_double]),
+    "pdhg_start": (C.c_int, [C.c_void_p, _dp, _dp]),
+    "pdhg_iterate": (C.c_int, [C.c_void_p, C.c_int]),
+    "pdhg_eval": (C.c_int, [C.c_void_p, C.c_int, C.c_double, _dp]),
+    "pdhg_eval_pair": (C.c_int, [C.c_void_p, C.c_double, _dp, _dp]),
+    "pdhg_restart": (C.c_int, [C.c_void_p, C.c_int, C.c_double]),
+    "pdhg_download": (C.c_int, [C.c_void_p, C.c_int, C.c_double, _dp, _dp]),
+    "pdhg_info": (C.c_int, [C.c_void_p, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]),
+    "pdhg_kernel_launches": (C.c_int64, [C.c_void_p]),
+    "pdhg_last_error": (C.c_char_p, [C.c_void_p]),
+    "pdhg_destroy": (None, [C.c_void_p]),
+    "taral_options_default": (None, [C.POINTER(OptionsT)]),
+    "taral_pdhg_input_error": (C.c_char_p, [C.POINTER(ModelT)]),
+    "taral_pdhg_solve": (C.c_int, [C.POINTER(ModelT), C.POINTER(OptionsT), C.POINTER(OutcomeT), _dp, _dp]),
+    "taral_pdhg_solve_warm": (C.c_int, [C.POINTER(ModelT), C.POINTER(OptionsT), _dp, _dp, C.POINTER(OutcomeT),
+                                        _dp, _dp]),
+    "taral_mps_read": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),
+    "taral_mps_error": (C.c_char_p, []),
+    "taral_mps_model": (C.c_int, [C.c_void_p, C.POINTER(ModelT)]),
+    "taral_mps_col_name": (C.c_char_p, [C.c_void_p, C.c_int]),
+    "taral_mps_row_name": (C.c_char_p, [C.c_void_p, C.c_int]),
+    "taral_mps_name": (C.c_char_p, [C.c_void_p]),
+    "taral_mps_free": (None, [C.c_void_p]),
+    "taral_spmv_plan_create": (C.c_int, [C.c_int, C.c_int, _lp, C.c_int, C.POINTER(C.c_void_p)]),
+    "taral_spmv_run": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                 C.c_void_p]),
+    "taral_spmv_plan_blocks": (C.c_int, [C.c_void_p]),
+    "taral_spmv_plan_destroy": (None, [C.c_void_p]),
+}
+
+_lib = None
+
+
+def lib():
+    """Load lib/libtaral_pdhg.so (raises if it is missing: build it with taral-lp_b200/build.py)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"{LIB_PATH} is missing: the CUDA engine has not been built (run build.py)")
+        L = C.CDLL(str(LIB_PATH))
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype, f.argtypes = res, args
+        _lib = L
+    return _lib
+
+
+def _check(code, ctx=None):
+    if code != OK:
+        msg = lib().pdhg_last_error(ctx).decode() if ctx else ""
+        raise TaralError(code, msg)
+
+
+def _p(a, t=_dp):
+    return a.ctypes.data_as(t)
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, np.float64)
+
+
+class _Csr:
+    def __init__(self, ptr, idx, val, cols):
+        self.ptr = np.ascontiguousarray(ptr, np.int64)
+        self.idx = np.ascontiguousarray(idx, np.int32)
+        self.val = _f64(val)
+        self.s = CsrT(len(self.ptr) - 1, cols, len(self.idx), _p(self.ptr, _lp), _p(self.idx, _ip), _p(self.val))
+
+
+class _Model:
+    """C view of a column-wise model (anything with the LP attributes of lpgen.LP); keeps the arrays alive."""
+
+    def __init__(self, lp):
+        self.a = dict(col_ptr=np.ascontiguousarray(lp.col_ptr, np.int64),
+                      row_idx=np.ascontiguousarray(lp.row_idx, np.int32),
+                      **{k: _f64(getattr(lp, k)) for k in ("val", "cost", "col_lo", "col_up", "row_lo", "row_up")})
+        is_int = getattr(lp, "is_int", None)
+        self.is_int = None if is_int is None else np.ascontiguousarray(is_int, np.uint8)
+        a = self.a
+        self.s = ModelT(int(lp.m), int(lp.n), _p(a["col_ptr"], _lp), _p(a["row_idx"], _ip), _p(a["val"]),
+                        _p(a["cost"]), _p(a["col_lo"]), _p(a["col_up"]), _p(a["row_lo"]), _p(a["row_up"]),
+                        float(getattr(lp, "obj_const", 0.0)), int(bool(getattr(lp, "maximize", False))),
+                        None if self.is_int is None else _p(self.is_int, _ubp),
+                        int(getattr(lp, "n_quadratic", 0)))
+
+
+# ------------------------------------------------------------------------------------------------ backend concept
+class Engine:
+    """Device context over a scaled problem (A_s, A_s^T and the 7 scaled vectors)."""
+
+    def __init__(self, A, AT, c, l, u, rl, ru, Dr, Dc, precision=FP64, eval_freq=64, graph=True):
+        m, n = len(A[0]) - 1, len(AT[0]) - 1
+        self.m, self.n = m, n
+        a, at = _Csr(*A, cols=n), _Csr(*AT, cols=m)
+        vecs = [_f64(v) for v in (c, l, u, rl, ru, Dr, Dc)]
+        h = C.c_void_p()
+        code = lib().pdhg_create(C.byref(a.s), C.byref(at.s), *[_p(v) for v in vecs], m, n, int(precision),
+                                 int(eval_freq), 0 if graph else 1, C.byref(h))
+        _check(code)
+        self.h = h
+
+    @classmethod
+    def from_scaled(cls, sp, **kw):
+        """From an object with A, AT (ptr, idx, val) tuples and c, l, u, rl, ru, Dr, Dc arrays."""
+        return cls(sp.A, sp.AT, sp.c, sp.l, sp.u, sp.rl, sp.ru, sp.Dr, sp.Dc, **kw)
+
+    def power_norm(self, iters=200):
+        v = C.c_double()
+        _check(lib().pdhg_power_norm(self.h, iters, C.byref(v)), self.h)
+        return v.value
+
+    def set_steps(self, tau, sigma):
+        _check(lib().pdhg_set_steps(self.h, tau, sigma), self.h)
+
+    def start(self, x0=None, z0=None):
+        x0 = None if x0 is None else _f64(x0)
+        z0 = None if z0 is None else _f64(z0)
+        _check(lib().pdhg_start(self.h, None if x0 is None else _p(x0), None if z0 is None else _p(z0)), self.h)
+
+    def iterate(self, steps):
+        _check(lib().pdhg_iterate(self.h, int(steps)), self.h)
+
+    def eval(self, avg, f):
+        out = np.zeros(10)
+        _check(lib().pdhg_eval(self.h, int(avg), float(f), _p(out)), self.h)
+        return out
+
+    def eval_pair(self, f):
+        cur, avg = np.zeros(10), np.zeros(10)
+        _check(lib().pdhg_eval_pair(self.h, float(f), _p(cur), _p(avg)), self.h)
+        return cur, avg
+
+    def restart(self, avg, f):
+        _check(lib().pdhg_restart(self.h, int(avg), float(f)), self.h)
+
+    def download(self, avg, f):
+        x, z = np.zeros(max(self.n, 1)), np.zeros(max(self.m, 1))
+        _check(lib().pdhg_download(self.h, int(avg), float(f), _p(x), _p(z)), self.h)
+        return x[:self.n], z[:self.m]
+
+    def info(self):
+        buf = C.create_string_buffer(256)
+        mem = C.c_size_t()
+        _check(lib().pdhg_info(self.h, buf, 256, C.byref(mem)), self.h)
+        return buf.value.decode(), mem.value
+
+    @property
+    def kernel_launches(self):
+        return lib().pdhg_kernel_launches(self.h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().pdhg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ------------------------------------------------------------------------------------------------ whole solve
+def default_options():
+    o = OptionsT()
+    lib().taral_options_default(C.byref(o))
+    return o
+
+
+def input_error(lp) -> Optional[str]:
+    r = lib().taral_pdhg_input_error(C.byref(_Model(lp).s))
+    return None if r is None else r.decode()
+
+
+def solve(lp, tol=1e-4, time_limit=3600.0, max_iter=2_000_000_000, eval_freq=64, row_rel=0.0, precision=FP64,
+          graph=True, verbose=False, x0=None, y0=None):
+    """Solve one LP on the GPU. Returns (outcome dict, x (n, original space), y (m, y = Dr z)).
+
+    x0 / y0: optional warm start in the original space (y in the minimisation form of the dual output)."""
+    mr = _Model(lp)
+    o = OptionsT(tol, time_limit, max_iter, eval_freq, row_rel, int(verbose), int(graph), int(precision))
+    r = OutcomeT()
+    x, y = np.zeros(max(lp.n, 1)), np.zeros(max(lp.m, 1))
+    if x0 is None and y0 is None:
+        code = lib().taral_pdhg_solve(C.byref(mr.s), C.byref(o), C.byref(r), _p(x), _p(y))
+    else:
+        xa = None if x0 is None else _f64(x0)
+        ya = None if y0 is None else _f64(y0)
+        code = lib().taral_pdhg_solve_warm(C.byref(mr.s), C.byref(o), None if xa is None else _p(xa),
+                                           None if ya is None else _p(ya), C.byref(r), _p(x), _p(y))
+    _check(code)
+    out = {k: getattr(r, k) for k, _ in OutcomeT._fields_}
+    out["status"] = STATUS[r.status]
+    return out, x[:lp.n], y[:lp.m]
+
+
+# ------------------------------------------------------------------------------------------------ MPS
+class MpsModel:
+    """A model read by the engine's MPS reader: numpy copies of the arrays plus row/column names."""
+
+    def __init__(self, path):
+        h = C.c_void_p()
+        code = lib().taral_mps_read(str(path).encode(), C.byref(h))
+        if code != OK:
+            raise TaralError(code, (lib().taral_mps_error() or b"").decode())
+        try:
+            v = ModelT()
+            _check(lib().taral_mps_model(h, C.byref(v)))
+            self.m, self.n = v.m, v.n
+            nnz = v.col_ptr[v.n] if v.n else 0
+
+            def arr(p, k, dt):
+                return np.ctypeslib.as_array(p, shape=(max(k, 1),))[:k].astype(dt, copy=True) if k else np.zeros(0, dt)
+            self.col_ptr = np.ctypeslib.as_array(v.col_ptr, shape=(v.n + 1,)).astype(np.int64, copy=True)
+            self.row_idx = arr(v.row_idx, nnz, np.int32)
+            self.val = arr(v.val, nnz, np.float64)
+            self.cost, self.col_lo, self.col_up = (arr(getattr(v, k), v.n, np.float64) for k in ("cost", "col_lo", "col_up"))
+            self.row_lo, self.row_up = (arr(getattr(v, k), v.m, np.float64) for k in ("row_lo", "row_up"))
+            self.obj_const, self.maximize = v.obj_const, bool(v.maximize)
+            self.is_int = arr(v.is_int, v.n, np.uint8)
+            self.n_quadratic = v.n_quadratic
+            self.name = (lib().taral_mps_name(h) or b"").decode()
+            self.col_names = [lib().taral_mps_col_name(h, j).decode() for j in range(v.n)]
+            self.row_names = [lib().taral_mps_row_name(h, i).decode() for i in range(v.m)]
+        finally:
+            lib().taral_mps_free(h)
+
+    @property
+    def nnz(self):
+        return int(self.col_ptr[-1])
+
+
+def read_mps(path) -> MpsModel:
+    return MpsModel(path)
+
+
+# ------------------------------------------------------------------------------------------------ SpMV
+class SpmvPlan:
+    """Row-block plan of a CSR matrix for y = A x on device buffers (int32 ptr/idx, float32 or float64 val)."""
+
+    def __init__(self, host_ptr, cols, dtype=FP32):
+        ptr = np.ascontiguousarray(host_ptr, np.int64)
+        h = C.c_void_p()
+        _check(lib().taral_spmv_plan_create(len(ptr) - 1, int(cols), _p(ptr, _lp), int(dtype), C.byref(h)))
+        self.h = h
+
+    @property
+    def blocks(self):
+        return lib().taral_spmv_plan_blocks(self.h)
+
+    def run(self, d_ptr, d_idx, d_val, d_x, d_y, stream=0):
+        """Device pointers as ints (e.g. torch tensor .data_ptr()); stream: cudaStream_t as int (0 = default)."""
+        _check(lib().taral_spmv_run(self.h, C.c_void_p(d_ptr), C.c_void_p(d_idx), C.c_void_p(d_val),
+                                    C.c_void_p(d_x), C.c_void_p(d_y), C.c_void_p(stream or None)))
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().taral_spmv_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def header_symbols(header: Path = PKG.parent / "include" / "taral_pdhg.h"):
+    """Function names declared in the C header (for the export check)."""
+    import re
+    text = header.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b((?:pdhg|taral)_[a-z0-9_]+)\s*\(", text)))

@@ -1,0 +1,119 @@
+#!/usr/bin/env python3
+"""Regenerate the golden fixtures of tests/golden/ from the reference implementation.
+
+Needs the reference checkout (REF, default /root/reference) and the reference binaries built from it by
+``make -C oracle ref`` (oracle/_ref/pdhg, oracle/_ref/taral). Writes:
+
+* gen_lp_sha256.json     sha256 of the MPS text that the reference's gpu/gen_lp.py writes for a few seeds
+* ledger_pins.json       the reference's published CPU-FP64 PDHG rows for packing_10000 and transport_100x100
+                         (results/gpu_pdhg/synth_*_tol1e-{4,6}.csv), read from its ledgers
+* reference_runs.json    reference `pdhg --device cpu --threads 1` (FP64) reports on generated models
+* reference_vectors.npz  the .sol / .dual vectors of those runs
+* reference_optima.json  the reference IPM optimum (`taral --method ipm`) of the planted 2000 x 5000 model
+
+Run from the repository root: python tests/golden/make_golden.py
+"""
+import csv
+import hashlib
+import json
+import os
+import subprocess
+import sys
+import tempfile
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+REF = Path(os.environ.get("REF", "/root/reference"))
+OUT = Path(__file__).resolve().parent
+PDHG = ROOT / "oracle" / "_ref" / "pdhg"
+TARAL = ROOT / "oracle" / "_ref" / "taral"
+sys.path.insert(0, str(ROOT / "taral-lp_b200"))
+import lpgen  # noqa: E402
+
+GEN_CASES = [("packing", ["10000"], 1), ("packing", ["2000"], 3), ("transport", ["100", "100"], 1),
+             ("transport", ["30", "40"], 2)]
+
+# (case name, model factory, pdhg flags)
+RUNS = [
+    ("packing_2000_s3_tol1e-4", lambda: lpgen.packing(2000, seed=3), ["--tol", "1e-4"]),
+    ("packing_2000_s3_tol1e-6", lambda: lpgen.packing(2000, seed=3), ["--tol", "1e-6"]),
+    ("transport_30x40_s2_tol1e-6", lambda: lpgen.transport(30, 40, seed=2), ["--tol", "1e-6"]),
+    ("planted_300x700_s5_tol1e-6", lambda: lpgen.planted(300, 700, 5, seed=5), ["--tol", "1e-6"]),
+    ("general_300x700_s3_tol1e-6", lambda: lpgen.general(300, 700, seed=3), ["--tol", "1e-6"]),
+    ("general_300x700_s3_max_tol1e-6", lambda: lpgen.general(300, 700, seed=3, maximize=True), ["--tol", "1e-6"]),
+    ("general_200x500_s7_rowrel100_tol1e-4", lambda: lpgen.general(200, 500, seed=7),
+     ["--tol", "1e-4", "--row-rel", "100"]),
+    ("general_200x500_s7_freq32_maxit3000", lambda: lpgen.general(200, 500, seed=7),
+     ["--tol", "1e-9", "--eval-freq", "32", "--max-iter", "3000"]),
+]
+
+
+def sha(text):
+    return hashlib.sha256(text.encode()).hexdigest()
+
+
+def read_vec(path):
+    return np.array([float(line.rsplit(None, 1)[1]) for line in open(path)])
+
+
+def main():
+    if not PDHG.exists() or not TARAL.exists():
+        sys.exit("build the reference first: make -C oracle ref")
+    with tempfile.TemporaryDirectory() as td:
+        td = Path(td)
+        gen = {}
+        for fam, args, seed in GEN_CASES:
+            f = td / "g.mps"
+            subprocess.run([sys.executable, str(REF / "gpu" / "gen_lp.py"), fam, *args, str(f), "--seed", str(seed)],
+                           check=True)
+            gen[f"{fam}_{'x'.join(args)}_s{seed}"] = sha(f.read_text())
+        (OUT / "gen_lp_sha256.json").write_text(json.dumps(gen, indent=1) + "\n")
+
+        pins = {}
+        for tol in ("1e-4", "1e-6"):
+            for fam in ("packing", "transport"):
+                with open(REF / "results" / "gpu_pdhg" / f"synth_{fam}_tol{tol}.csv") as fh:
+                    for row in csv.DictReader(fh):
+                        if row["device"] == "cpu" and row["threads"] == "1" and row["case"] in (
+                                "packing_10000", "transport_100x100"):
+                            pins[f"{row['case']}_tol{tol}"] = {
+                                k: row[k] for k in ("case", "tol", "status", "objective", "iterations", "restarts",
+                                                    "rel_primal", "rel_dual", "rel_gap", "max_row_violation")}
+        (OUT / "ledger_pins.json").write_text(json.dumps(pins, indent=1) + "\n")
+
+        runs, vecs = {}, {}
+        for name, make, flags in RUNS:
+            lp = make()
+            f = td / "m.mps"
+            lp.write_mps(f)
+            j, s, d = td / "r.json", td / "r.sol", td / "r.dual"
+            subprocess.run([str(PDHG), str(f), "--device", "cpu", "--threads", "1", *flags, "--json", str(j),
+                            "--sol", str(s), "--dual", str(d)], check=True, stdout=subprocess.DEVNULL)
+            rep = json.loads(j.read_text())
+            runs[name] = {"flags": flags, "model_sha256": lp.digest(),
+                          **{k: rep[k] for k in ("status", "objective", "iterations", "restarts", "rel_primal",
+                                                 "rel_dual", "rel_gap", "point", "max_row_violation",
+                                                 "max_bound_violation", "norm_a", "primal_weight", "rows", "cols",
+                                                 "nnz")}}
+            vecs[name + "/x"] = read_vec(s)
+            vecs[name + "/y"] = read_vec(d)
+        (OUT / "reference_runs.json").write_text(json.dumps(runs, indent=1) + "\n")
+        np.savez_compressed(OUT / "reference_vectors.npz", **vecs)
+
+        lp = lpgen.planted(2000, 5000, 5, seed=0)
+        f = td / "p.mps"
+        lp.write_mps(f)
+        j = td / "p.json"
+        subprocess.run([str(TARAL), str(f), "--method", "ipm", "--time-limit", "600", "--json", str(j)], check=True,
+                       stdout=subprocess.DEVNULL)
+        rep = json.loads(j.read_text())
+        opt = {"planted_2000x5000_s0": {"method": "ipm", "status": rep.get("status"), "objective": rep.get("objective"),
+                                         "planted_objective": lp.obj_star, "model_sha256": lp.digest()}}
+        (OUT / "reference_optima.json").write_text(json.dumps(opt, indent=1) + "\n")
+    print("wrote", sorted(p.name for p in OUT.iterdir()))
+
+
+if __name__ == "__main__":
+    main()

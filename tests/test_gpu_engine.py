@@ -1,0 +1,145 @@
+"""Step-level parity of the CUDA engine with the CPU oracle (backend concept of gpu/pdhg.cu:313-514).
+
+Both sides start from the same scaled problem (the oracle's scaling) and execute the same calls; FP64 results
+must agree to rounding (different summation orders), FP32 results to single precision."""
+import numpy as np
+import pytest
+
+import lpgen
+import oracle
+import pdhg
+
+pytestmark = pytest.mark.gpu
+
+CASES = {
+    "packing_2000": lambda: lpgen.packing(2000, seed=3),
+    "transport_30x40": lambda: lpgen.transport(30, 40, seed=2),
+    "general_300x700": lambda: lpgen.general(300, 700, seed=3),
+    "planted_zipf": lambda: lpgen.planted(3000, 6000, 8, seed=1, zipf=1.2, cap=3000),
+}
+
+
+def _pair(lp, precision=pdhg.FP64):
+    sp = oracle.ScaledProblem(lp)
+    eng = pdhg.Engine.from_scaled(sp, precision=precision)
+    ref = oracle.Stepper(sp)
+    return sp, eng, ref
+
+
+def _close(a, b, rtol, atol=1e-300):
+    a, b = np.asarray(a), np.asarray(b)
+    scale = np.maximum(np.abs(b), 1.0)
+    return np.all(np.abs(a - b) <= rtol * scale + atol)
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_power_norm_fp64(engine_lib, oracle_lib, case):
+    sp, eng, _ = _pair(CASES[case]())
+    assert abs(eng.power_norm(200) - sp.power_norm(200)) <= 1e-12 * sp.power_norm(200)
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_steps_match_oracle_fp64(engine_lib, oracle_lib, case):
+    """start -> eval -> 3 blocks of 64 steps with a restart to the average and one to the current point."""
+    sp, eng, ref = _pair(CASES[case]())
+    norm = sp.power_norm(200)
+    tau = sigma = 0.95 / norm
+    for b in (eng, ref):
+        b.set_steps(tau * 0.7, sigma / 0.7)
+        b.start()
+    assert _close(eng.eval(0, 1.0), ref.eval(0, 1.0), 1e-11)
+    for blk, action in enumerate(("avg", "cur", None)):
+        for b in (eng, ref):
+            b.iterate(64)
+        f = 1.0 / 64
+        cur, avg = eng.eval_pair(f)
+        assert _close(cur, ref.eval(0, 1.0), 1e-9), (blk, cur, ref.eval(0, 1.0))
+        assert _close(avg, ref.eval(1, f), 1e-9), (blk, avg, ref.eval(1, f))
+        xg, zg = eng.download(1, f)
+        xo, zo = ref.download(1, f)
+        assert _close(xg, xo, 1e-9) and _close(zg, zo, 1e-9)
+        if action:
+            for b in (eng, ref):
+                b.restart(action == "avg", f)
+    xg, zg = eng.download(0, 1.0)
+    xo, zo = ref.download(0, 1.0)
+    assert _close(xg, xo, 1e-9) and _close(zg, zo, 1e-9)
+
+
+@pytest.mark.parametrize("case", ["packing_2000", "general_300x700"])
+def test_steps_fp32_track_fp64(engine_lib, oracle_lib, case):
+    """FP32 iterates follow the FP64 trajectory to single-precision accuracy over one block."""
+    sp, eng, ref = _pair(CASES[case](), pdhg.FP32)
+    norm = sp.power_norm(200)
+    for b in (eng, ref):
+        b.set_steps(0.95 / norm, 0.95 / norm)
+        b.start()
+        b.iterate(64)
+    xg, zg = eng.download(1, 1 / 64)
+    xo, zo = ref.download(1, 1 / 64)
+    assert _close(xg, xo, 1e-4) and _close(zg, zo, 1e-4)
+
+
+def test_deterministic(engine_lib, oracle_lib):
+    """Fixed-order reductions: two contexts give bit-identical KKT scalars and iterates."""
+    lp = CASES["planted_zipf"]()
+    outs = []
+    for _ in range(2):
+        sp, eng, _ = _pair(lp)
+        eng.set_steps(0.5, 0.5)
+        eng.start()
+        eng.iterate(64)
+        outs.append((eng.eval_pair(1 / 64), eng.download(0, 1.0)))
+    (c1, a1), (x1, z1) = outs[0]
+    (c2, a2), (x2, z2) = outs[1]
+    assert np.array_equal(c1, c2) and np.array_equal(a1, a2) and np.array_equal(x1, x2) and np.array_equal(z1, z2)
+
+
+def test_graph_and_direct_launch_agree(engine_lib, oracle_lib):
+    lp = CASES["general_300x700"]()
+    sp = oracle.ScaledProblem(lp)
+    res = []
+    for graph in (True, False):
+        eng = pdhg.Engine.from_scaled(sp, graph=graph)
+        eng.set_steps(0.4, 0.6)
+        eng.start()
+        eng.iterate(64)
+        eng.iterate(64)
+        res.append(eng.download(0, 1.0))
+    assert np.array_equal(res[0][0], res[1][0]) and np.array_equal(res[0][1], res[1][1])
+
+
+def test_warm_start_point(engine_lib, oracle_lib):
+    lp = CASES["general_300x700"]()
+    sp = oracle.ScaledProblem(lp)
+    eng = pdhg.Engine.from_scaled(sp)
+    rng = np.random.default_rng(0)
+    x0, z0 = rng.standard_normal(sp.n), rng.standard_normal(sp.m)
+    eng.set_steps(0.5, 0.5)
+    eng.start(x0, z0)
+    x, z = eng.download(0, 1.0)
+    assert np.array_equal(x, x0) and np.array_equal(z, z0)
+
+
+def test_state_errors(engine_lib, oracle_lib):
+    sp = oracle.ScaledProblem(CASES["packing_2000"]())
+    eng = pdhg.Engine.from_scaled(sp)
+    with pytest.raises(pdhg.TaralError) as e:
+        eng.iterate(8)
+    assert e.value.code == pdhg.ERR_STATE
+    bad_idx = sp.A[1].copy()
+    bad_idx[-1] = sp.n  # a column index out of range is rejected before anything reaches the device
+    with pytest.raises(pdhg.TaralError) as e:
+        pdhg.Engine((sp.A[0], bad_idx, sp.A[2]), sp.AT, sp.c, sp.l, sp.u, sp.rl, sp.ru, sp.Dr, sp.Dc)
+    assert e.value.code == pdhg.ERR_INPUT
+
+
+def test_kernel_launch_count(engine_lib, oracle_lib):
+    sp = oracle.ScaledProblem(CASES["packing_2000"]())
+    eng = pdhg.Engine.from_scaled(sp)
+    eng.set_steps(0.5, 0.5)
+    eng.start()
+    before = eng.kernel_launches
+    eng.iterate(64)
+    eng.iterate(64)
+    assert eng.kernel_launches - before == 2 * (1 + 2 * 64)
