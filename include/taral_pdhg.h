@@ -146,6 +146,7 @@ typedef struct {
     size_t device_mem_bytes;
     int64_t kernel_launches;
     int64_t nnz;
+    double device_s;        /* pdhg_solve_ctx: CUDA-event time of the solve on the context stream */
 } taral_outcome;
 
 void taral_options_default(taral_options* o);
@@ -161,6 +162,22 @@ int taral_pdhg_solve(const taral_model* md, const taral_options* o, taral_outcom
  * restart across solves is the simplex crossover of src/crossover.cpp:15-60). */
 int taral_pdhg_solve_warm(const taral_model* md, const taral_options* o, const double* x0, const double* y0,
                           taral_outcome* out, double* x_out, double* y_out);
+
+/* Backend-level entries that take the solver's options and outcome types. */
+/* Input gate + scaling (gpu/pdhg.cu:80-133) + pdhg_create for a column-wise model: the device context of the
+ * model's scaled problem. bnorm / cnorm (may be NULL) receive the original-space norms pdhg_solve_ctx needs. */
+int pdhg_create_model(const taral_model* md, int precision, int eval_freq, unsigned flags, pdhg_ctx** out,
+                      double* bnorm, double* cnorm);
+/* run<B> (gpu/pdhg.cu:761-849) on an existing context: power iteration, step sizes, the eval / terminate /
+ * restart loop and the final download (x, z in the scaled space; either may be NULL). bnorm and cnorm are the
+ * original-space norms of the stopping test (gpu/pdhg.cu:118-131); c, rl, ru are the ones given at creation.
+ * x0 / z0: optional start point (scaled space). out->device_s is the device time of the whole solve. */
+int pdhg_solve_ctx(pdhg_ctx* ctx, double bnorm, double cnorm, const taral_options* o, const double* x0,
+                   const double* z0, taral_outcome* out, double* x, double* z);
+/* Measurement hook: `reps` iterations launched kernel by kernel, each row-phase (A x + dual step) and
+ * column-phase (A^T z + primal step) kernel bracketed by CUDA events on the context stream. Returns the mean
+ * milliseconds per launch of each. Advances the iteration state like pdhg_iterate(ctx, reps). */
+int pdhg_profile_phases(pdhg_ctx* ctx, int reps, double* row_ms, double* col_ms);
 
 /* ------------------------------------------------------------------------------------------------------------
  * 3. Problem format. Replaces read_mps (src/taral.hpp:48, src/mps.cpp:388-399): free format first, fixed
@@ -191,6 +208,28 @@ int taral_spmv_run(const taral_spmv_plan* plan, const int32_t* d_ptr, const int3
                    const void* d_x, void* d_y, void* stream);
 int taral_spmv_plan_blocks(const taral_spmv_plan* plan);
 void taral_spmv_plan_destroy(taral_spmv_plan* plan);
+
+/* ------------------------------------------------------------------------------------------------------------
+ * 5. Batched solve: many LPs of one scenario family in one context (SURVEY: the batched scenario family). No
+ *    counterpart in the reference, which solves one model per process (gpu/pdhg.cu:937-992); each instance
+ *    follows the reference driver's rules (gpu/pdhg.cu:761-849) with its own step sizes, primal weight,
+ *    restarts and stopping, evaluated on the device so a block of eval_freq iterations for the whole batch is
+ *    one CUDA graph. Instances with identical constraint matrices share one scaled copy of A and A^T.
+ * ------------------------------------------------------------------------------------------------------------ */
+typedef struct taral_batch taral_batch;
+/* Scale every model (matrices shared where identical) and upload the batch. The models and the arrays they
+ * point into must stay valid until taral_batch_destroy (the final original-space check reads them). */
+int taral_batch_create(const taral_model* models, int count, const taral_options* o, taral_batch** out);
+/* Solve all instances. x0[i] / y0[i]: optional warm start of instance i (original space, y in the minimisation
+ * form), x0 / y0 themselves may be NULL. outs[i]: instance i's outcome (solve_s and device_s are the whole
+ * batch's). x_out[i] (n_i) / y_out[i] (m_i) may be NULL, as may x_out / y_out. */
+int taral_batch_solve(taral_batch* b, const double* const* x0, const double* const* y0, taral_outcome* outs,
+                      double* const* x_out, double* const* y_out);
+/* Distinct stored matrices, device bytes, nonzeros stored and nonzeros over all instances. */
+int taral_batch_info(const taral_batch* b, int* distinct_matrices, size_t* device_mem, int64_t* nnz_stored,
+                     int64_t* nnz_total);
+const char* taral_batch_last_error(const taral_batch* b);
+void taral_batch_destroy(taral_batch* b);
 
 #ifdef __cplusplus
 }

@@ -22,27 +22,32 @@
 
 #include "../../include/taral_pdhg.h"
 #include "engine.hpp"
+#include "host.hpp"
 #include "kernels.cuh"
 
 namespace taral {
 
 // ---------------------------------------------------------------------------------------------- row blocks
-std::vector<int> build_row_blocks(const int64_t* ptr, int rows) {
-    std::vector<int> b{0};
-    int cur_rows = 0;
+// Consecutive rows are packed into blocks of at most kTile nonzeros and kRowsMax rows; a longer row is a block of
+// its own (block_sums sums it with the whole CTA).
+std::vector<int4> build_row_blocks(const int64_t* ptr, int rows) {
+    std::vector<int4> out;
+    auto close = [&](int r0, int r1) { out.push_back(make_int4(r0, r1 - r0, int(ptr[r0]), int(ptr[r1]))); };
+    int start = 0, cur_rows = 0;
     int64_t cur_nnz = 0;
     for (int r = 0; r < rows; ++r) {
         int64_t L = ptr[r + 1] - ptr[r];
         if (L > kTile) {  // a long row is a block of its own
-            if (cur_rows) b.push_back(r), cur_rows = 0, cur_nnz = 0;
-            b.push_back(r + 1);
+            if (cur_rows) close(start, r);
+            close(r, r + 1);
+            start = r + 1, cur_rows = 0, cur_nnz = 0;
             continue;
         }
-        if (cur_rows == kRowsMax || cur_nnz + L > kTile) b.push_back(r), cur_rows = 0, cur_nnz = 0;
+        if (cur_rows == kRowsMax || cur_nnz + L > kTile) close(start, r), start = r, cur_rows = 0, cur_nnz = 0;
         ++cur_rows, cur_nnz += L;
     }
-    if (cur_rows) b.push_back(rows);
-    return b;
+    if (cur_rows) close(start, rows);
+    return out;
 }
 
 static int grid_for(int64_t k) {  // elementwise kernels: grid-stride, at most 8 CTAs of 256 per SM
@@ -66,7 +71,8 @@ struct CudaError {
 struct DevMat {
     int rows = 0;
     int64_t nnz = 0;
-    int *ptr = nullptr, *idx = nullptr, *blk = nullptr;
+    int *ptr = nullptr, *idx = nullptr;
+    int4* blk = nullptr;
     void* val = nullptr;
     int nblk = 0;
 };
@@ -76,8 +82,8 @@ struct Engine final : EngineBase {
     int m = 0, n = 0, eval_freq = 64;
     bool use_graph = true;
     DevMat A, AT;
-    T *c = nullptr, *l = nullptr, *u = nullptr, *rl = nullptr, *ru = nullptr, *Dr = nullptr, *Dc = nullptr,
-      *par = nullptr;
+    T *c = nullptr, *l = nullptr, *u = nullptr, *rl = nullptr, *ru = nullptr, *Dr = nullptr, *Dc = nullptr;
+    double* par = nullptr;  // {tau, sigma}
     T *x = nullptr, *z = nullptr, *Ax = nullptr, *ATz = nullptr, *xlast = nullptr, *zlast = nullptr;
     T *pv = nullptr, *pw = nullptr, *pu = nullptr;
     double *xs = nullptr, *zs = nullptr, *tmp_m = nullptr, *tmp_n = nullptr, *hbuf = nullptr, *part = nullptr,
@@ -116,18 +122,19 @@ struct Engine final : EngineBase {
         d.rows = a.rows, d.nnz = a.nnz;
         std::vector<int> p32(size_t(a.rows) + 1);
         for (int r = 0; r <= a.rows; ++r) p32[r] = int(a.ptr[r]);
-        std::vector<int> blk = build_row_blocks(a.ptr, a.rows);
-        d.nblk = int(blk.size()) - 1;
-        d.ptr = alloc<int>(p32.size()), d.idx = alloc<int>(size_t(a.nnz)), d.blk = alloc<int>(blk.size());
+        std::vector<int4> blk = build_row_blocks(a.ptr, a.rows);
+        d.nblk = int(blk.size());
+        d.ptr = alloc<int>(p32.size()), d.idx = alloc<int>(size_t(a.nnz)), d.blk = alloc<int4>(blk.size());
         CK(cudaMemcpyAsync(d.ptr, p32.data(), p32.size() * sizeof(int), cudaMemcpyHostToDevice, st));
         if (a.nnz) CK(cudaMemcpyAsync(d.idx, a.idx, size_t(a.nnz) * sizeof(int), cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(d.blk, blk.data(), blk.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+        if (!blk.empty())
+            CK(cudaMemcpyAsync(d.blk, blk.data(), blk.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
         d.val = upload(a.val, size_t(a.nnz));
         return d;
     }
 
-    void init(const taral_csr& hA, const taral_csr& hAT, const double* hc, const double* hl, const double* hu,
-              const double* hrl, const double* hru, const double* hDr, const double* hDc, int m_, int n_,
+    void init(const taral_csr& hA, const taral_csr& hAT, const double* hc_ptr, const double* hl, const double* hu,
+              const double* hrl_ptr, const double* hru_ptr, const double* hDr, const double* hDc, int m_, int n_,
               int freq, unsigned flags) {
         m = m_, n = n_, eval_freq = std::max(1, freq), use_graph = !(flags & TARAL_FLAG_NO_GRAPH);
         size_t free0, free1, total;
@@ -139,9 +146,9 @@ struct Engine final : EngineBase {
         name = prop.name;
         CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
         A = upload(hA), AT = upload(hAT);
-        c = upload(hc, n), l = upload(hl, n), u = upload(hu, n), Dc = upload(hDc, n);
-        rl = upload(hrl, m), ru = upload(hru, m), Dr = upload(hDr, m);
-        par = zeros<T>(2);
+        c = upload(hc_ptr, n), l = upload(hl, n), u = upload(hu, n), Dc = upload(hDc, n);
+        rl = upload(hrl_ptr, m), ru = upload(hru_ptr, m), Dr = upload(hDr, m);
+        par = zeros<double>(2);
         x = zeros<T>(n), ATz = zeros<T>(n), xlast = zeros<T>(n);
         z = zeros<T>(m), Ax = zeros<T>(m), zlast = zeros<T>(m);
         xs = zeros<double>(n), zs = zeros<double>(m), tmp_n = zeros<double>(n), tmp_m = zeros<double>(m);
@@ -153,6 +160,7 @@ struct Engine final : EngineBase {
         pst = zeros<double>(4);
         tickets = zeros<unsigned>(4);
         pdone = zeros<int>(1);
+        hc.assign(hc_ptr, hc_ptr + n), hrl.assign(hrl_ptr, hrl_ptr + m), hru.assign(hru_ptr, hru_ptr + m);
         CK(cudaMallocHost(&h_out, 32 * sizeof(double)));
         CK(cudaMallocHost(&h_flag, sizeof(int)));
         CK(cudaStreamSynchronize(st));
@@ -160,6 +168,7 @@ struct Engine final : EngineBase {
         mem_used = free0 - free1;
     }
     ~Engine() override {
+        if (ev0) cudaEventDestroy(ev0), cudaEventDestroy(ev1);
         if (graph) cudaGraphExecDestroy(graph);
         if (st) cudaStreamSynchronize(st);
         for (void* p : allocs) cudaFree(p);
@@ -220,7 +229,7 @@ struct Engine final : EngineBase {
         return h_out[0];
     }
     void set_steps(double tau, double sigma) override {
-        k_set_par<T><<<1, 1, 0, st>>>(par, T(tau), T(sigma));
+        k_set_par<<<1, 1, 0, st>>>(par, tau, sigma);
         ++launches;
         CK(cudaGetLastError());
     }
@@ -327,6 +336,45 @@ struct Engine final : EngineBase {
         CK(cudaGetLastError());
     }
     void sync() override { CK(cudaStreamSynchronize(st)); }
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    void mark() override {
+        if (!ev0) {
+            CK(cudaEventCreate(&ev0));
+            CK(cudaEventCreate(&ev1));
+        }
+        CK(cudaEventRecord(ev0, st));
+    }
+    double elapsed_ms() override {
+        CK(cudaEventRecord(ev1, st));
+        CK(cudaEventSynchronize(ev1));
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, ev0, ev1));
+        return ms;
+    }
+    void profile_phases(int reps, double* row_ms, double* col_ms) override {
+        std::vector<cudaEvent_t> ev(size_t(4) * reps);
+        for (auto& e : ev) CK(cudaEventCreate(&e));
+        k_xupd<T><<<grid_for(n), 256, 0, st>>>(n, x, ATz, c, l, u, par, xs);
+        ++launches;
+        for (int s = 0; s < reps; ++s) {
+            CK(cudaEventRecord(ev[4 * s], st));
+            rowblock(A, x, EpiRow<T>{Ax, z, zs, rl, ru, par});
+            CK(cudaEventRecord(ev[4 * s + 1], st));
+            CK(cudaEventRecord(ev[4 * s + 2], st));
+            rowblock(AT, z, EpiCol<T>{ATz, x, xs, c, l, u, par, s + 1 < reps ? 1 : 0});
+            CK(cudaEventRecord(ev[4 * s + 3], st));
+        }
+        CK(cudaStreamSynchronize(st));
+        double r = 0, c2 = 0;
+        for (int s = 0; s < reps; ++s) {
+            float a, b;
+            CK(cudaEventElapsedTime(&a, ev[4 * s], ev[4 * s + 1]));
+            CK(cudaEventElapsedTime(&b, ev[4 * s + 2], ev[4 * s + 3]));
+            r += a, c2 += b;
+        }
+        for (auto& e : ev) cudaEventDestroy(e);
+        *row_ms = r / reps, *col_ms = c2 / reps;
+    }
 };
 
 std::unique_ptr<EngineBase> make_engine(int precision) {
@@ -362,9 +410,9 @@ static int fail(pdhg_ctx* c, int code, const std::string& msg) {
     return code;
 }
 
-#define GUARD(ctx, body)                                                             \
+#define GUARD(ctx, ...)                                                              \
     try {                                                                            \
-        body;                                                                        \
+        __VA_ARGS__;                                                                 \
         return TARAL_OK;                                                             \
     } catch (const taral::CudaError& ex) {                                           \
         return fail(ctx, TARAL_ERR_CUDA, ex.msg);                                    \
@@ -452,6 +500,39 @@ extern "C" int pdhg_download(pdhg_ctx* ctx, int avg, double f, double* x, double
     if (!ctx || !x || !z) return TARAL_ERR_INPUT;
     GUARD(ctx, ctx->e->download(avg != 0, f, x, z))
 }
+extern "C" int pdhg_solve_ctx(pdhg_ctx* ctx, double bnorm, double cnorm, const taral_options* o, const double* x0,
+                              const double* z0, taral_outcome* out, double* x, double* z) {
+    if (!ctx || !o || !out) return TARAL_ERR_INPUT;
+    std::memset(out, 0, sizeof *out);
+    taral::Options op;
+    op.tol = o->tol, op.time_limit = o->time_limit, op.max_iter = o->max_iter;
+    op.eval_freq = o->eval_freq > 0 ? o->eval_freq : 64, op.row_rel = o->row_rel, op.verbose = o->verbose != 0;
+    EngineBase& e = *ctx->e;
+    taral::DriverData P{int(e.hrl.size()), int(e.hc.size()), e.hc.data(), e.hrl.data(), e.hru.data(), bnorm, cnorm};
+    GUARD(ctx, {
+        int64_t l0 = e.launches;
+        auto t0 = taral::Clock::now();
+        e.mark();
+        taral::Outcome r = taral::run(e, P, op, op.time_limit, x0, z0);
+        out->device_s = e.elapsed_ms() * 1e-3;
+        out->solve_s = taral::since(t0);
+        ctx->started = true;
+        out->status = r.status, out->iterations = r.iterations, out->restarts = r.restarts;
+        out->from_average = r.from_average ? 1 : 0;
+        out->rel_primal = r.rel_primal, out->rel_dual = r.rel_dual, out->rel_gap = r.rel_gap;
+        out->norm_a = r.norm_a, out->primal_weight = r.omega, out->power_iter_s = r.power_s;
+        out->device_mem_bytes = e.mem_used, out->kernel_launches = e.launches - l0;
+        if (x) std::memcpy(x, r.x.data(), r.x.size() * sizeof(double));
+        if (z) std::memcpy(z, r.z.data(), r.z.size() * sizeof(double));
+    })
+}
+
+extern "C" int pdhg_profile_phases(pdhg_ctx* ctx, int reps, double* row_ms, double* col_ms) {
+    if (!ctx || reps <= 0 || !row_ms || !col_ms) return TARAL_ERR_INPUT;
+    if (!ctx->started) return fail(ctx, TARAL_ERR_STATE, "pdhg_profile_phases before pdhg_start");
+    GUARD(ctx, ctx->e->profile_phases(reps, row_ms, col_ms))
+}
+
 extern "C" int pdhg_info(pdhg_ctx* ctx, char* name_out, size_t cap, size_t* mem_used) {
     if (!ctx) return TARAL_ERR_INPUT;
     if (name_out && cap) {
@@ -467,7 +548,7 @@ extern "C" void pdhg_destroy(pdhg_ctx* ctx) { delete ctx; }
 // ================================================================================================ SpMV plan
 struct taral_spmv_plan {
     int rows = 0, cols = 0, dtype = TARAL_FP64, nblk = 0;
-    int* blk = nullptr;
+    int4* blk = nullptr;
 };
 
 extern "C" int taral_spmv_plan_create(int rows, int cols, const int64_t* host_ptr, int dtype, taral_spmv_plan** out) {
@@ -477,14 +558,15 @@ extern "C" int taral_spmv_plan_create(int rows, int cols, const int64_t* host_pt
     for (int r = 0; r < rows; ++r)
         if (host_ptr[r + 1] < host_ptr[r]) return TARAL_ERR_INPUT;
     if (host_ptr[rows] > INT32_MAX - 64) return TARAL_ERR_INPUT;
-    std::vector<int> blk = taral::build_row_blocks(host_ptr, rows);
+    std::vector<int4> blk = taral::build_row_blocks(host_ptr, rows);
     auto* p = new taral_spmv_plan;
-    p->rows = rows, p->cols = cols, p->dtype = dtype, p->nblk = int(blk.size()) - 1;
-    if (cudaMalloc(&p->blk, blk.size() * sizeof(int)) != cudaSuccess) {
+    p->rows = rows, p->cols = cols, p->dtype = dtype, p->nblk = int(blk.size());
+    if (cudaMalloc(&p->blk, std::max<size_t>(blk.size(), 1) * sizeof(int4)) != cudaSuccess) {
         delete p;
         return TARAL_ERR_ALLOC;
     }
-    if (cudaMemcpy(p->blk, blk.data(), blk.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess) {
+    if (!blk.empty() &&
+        cudaMemcpy(p->blk, blk.data(), blk.size() * sizeof(int4), cudaMemcpyHostToDevice) != cudaSuccess) {
         cudaFree(p->blk);
         delete p;
         return TARAL_ERR_CUDA;

@@ -5,6 +5,8 @@
 #include <string>
 #include <vector>
 
+#include <vector_types.h>
+
 #include "../../include/taral_pdhg.h"
 
 namespace taral {
@@ -24,12 +26,20 @@ struct EngineBase {
     virtual void restart(bool avg, double f) = 0;
     virtual void download(bool avg, double f, double* x, double* z) = 0;
     virtual void sync() = 0;
+    // Device time on the context stream between mark() and elapsed_ms() (CUDA events).
+    virtual void mark() = 0;
+    virtual double elapsed_ms() = 0;
+    // `reps` PDHG iterations launched one kernel at a time, each row-phase and column-phase kernel bracketed by
+    // CUDA events on the context stream; average milliseconds per launch of each.
+    virtual void profile_phases(int reps, double* row_ms, double* col_ms) = 0;
+    // Host copies of the scaled c, rl, ru kept at creation (the driver's step-size and norm set-up reads them).
+    std::vector<double> hc, hrl, hru;
 };
 
 std::unique_ptr<EngineBase> make_engine(int precision);
 void engine_init(EngineBase& e, int precision, const taral_csr& A, const taral_csr& AT, const double* c,
                  const double* l, const double* u, const double* rl, const double* ru, const double* Dr,
                  const double* Dc, int m, int n, int eval_freq, unsigned flags);
-std::vector<int> build_row_blocks(const int64_t* ptr, int rows);
+std::vector<int4> build_row_blocks(const int64_t* ptr, int rows);
 
 }  // namespace taral

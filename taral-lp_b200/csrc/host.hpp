@@ -55,6 +55,11 @@ struct Scaled {
     double bnorm = 0, cnorm = 0;  // original-space norms of the stopping test
 };
 Scaled build_scaled(const taral_model& md, double sign);  // gpu/pdhg.cu:80-133
+// The two halves of build_scaled: the matrix part (A_s, A_s^T, Dr, Dc: depends on A only) and the vector part
+// (c, l, u, rl, ru and the original-space norms, given Dr and Dc). Instances that share A share the first.
+void scale_matrix(const taral_model& md, Scaled& P);
+void scale_vectors(const taral_model& md, double sign, const std::vector<double>& Dr, const std::vector<double>& Dc,
+                   Scaled& P);
 
 struct Options {  // gpu/pdhg.cu:744-750
     double tol = 1e-4, time_limit = 3600;
@@ -76,6 +81,14 @@ struct Outcome {  // gpu/pdhg.cu:752-759
 
 const char* status_name(int s);
 
+// What the driver reads of the scaled problem: sizes, c_s, [rl, ru]_s and the original-space norms.
+struct DriverData {
+    int m = 0, n = 0;
+    const double *c = nullptr, *rl = nullptr, *ru = nullptr;
+    double bnorm = 0, cnorm = 0;
+    static DriverData of(const Scaled& P) { return {P.m, P.n, P.c.data(), P.rl.data(), P.ru.data(), P.bnorm, P.cnorm}; }
+};
+
 // KKT scalar slots (gpu/pdhg.cu:136, 145).
 enum { PR2S, PR2O, PR2R, DROW, DZ2, DR2S, DR2O, POBJ, DCOL, DX2 };
 
@@ -84,7 +97,7 @@ enum { PR2S, PR2O, PR2R, DROW, DZ2, DR2S, DR2O, POBJ, DCOL, DX2 };
 // space). The stopping rule, restart rule and primal-weight update follow the reference line by line; the
 // KKT scalars of the current point and of the average come back together (one synchronisation per block).
 template <class B>
-Outcome run(B& b, const Scaled& P, const Options& o, double time_budget, const double* x0 = nullptr,
+Outcome run(B& b, const DriverData& P, const Options& o, double time_budget, const double* x0 = nullptr,
             const double* z0 = nullptr) {
     Outcome r;
     auto t0 = Clock::now();
@@ -92,7 +105,7 @@ Outcome run(B& b, const Scaled& P, const Options& o, double time_budget, const d
     r.power_s = since(t0);
     double eta = r.norm_a > 0 ? 0.95 / r.norm_a : 1.0;
     double cs = 0, bs = 0;
-    for (double v : P.c) cs += v * v;
+    for (int j = 0; j < P.n; ++j) cs += P.c[j] * P.c[j];
     for (int i = 0; i < P.m; ++i) {
         double lo = P.rl[i], up = P.ru[i];
         double v = std::isfinite(lo) && std::isfinite(up) ? std::max(std::fabs(lo), std::fabs(up))

@@ -18,7 +18,7 @@
 namespace taral {
 
 constexpr int kThreads = 256;  // threads per CTA in every SpMV-shaped kernel
-constexpr int kTile = 2048;    // nonzeros staged per row block
+constexpr int kTile = 2044;    // nonzeros staged per row block: with the 16-byte alignment slack, 512 quads
 constexpr int kRowsMax = 256;  // rows per row block (one epilogue row per thread)
 constexpr int kRedThreads = 256;
 
@@ -27,21 +27,23 @@ __device__ __forceinline__ T clampv(T v, T lo, T hi) { return v < lo ? lo : (v >
 
 // ------------------------------------------------------------------------------------------ vector loads
 template <class T> struct Quad;
+// The matrix is streamed once per phase: its 16-byte loads bypass L1 (no_allocate) so that L1 keeps the gathered
+// vector entries, which are reused across rows.
 template <> struct Quad<float> {
     __device__ __forceinline__ static void load(const float* p, float (&v)[4]) {
-        float4 q = __ldg(reinterpret_cast<const float4*>(p));
-        v[0] = q.x, v[1] = q.y, v[2] = q.z, v[3] = q.w;
+        asm volatile("ld.global.nc.L1::no_allocate.v4.f32 {%0,%1,%2,%3}, [%4];"
+                     : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]) : "l"(p));
     }
 };
 template <> struct Quad<double> {
     __device__ __forceinline__ static void load(const double* p, double (&v)[4]) {
-        double2 a = __ldg(reinterpret_cast<const double2*>(p)), b = __ldg(reinterpret_cast<const double2*>(p) + 1);
-        v[0] = a.x, v[1] = a.y, v[2] = b.x, v[3] = b.y;
+        asm volatile("ld.global.nc.L1::no_allocate.v2.f64 {%0,%1}, [%2];" : "=d"(v[0]), "=d"(v[1]) : "l"(p));
+        asm volatile("ld.global.nc.L1::no_allocate.v2.f64 {%0,%1}, [%2];" : "=d"(v[2]), "=d"(v[3]) : "l"(p + 2));
     }
 };
 __device__ __forceinline__ void load_idx4(const int* p, int (&v)[4]) {
-    int4 q = __ldg(reinterpret_cast<const int4*>(p));
-    v[0] = q.x, v[1] = q.y, v[2] = q.z, v[3] = q.w;
+    asm volatile("ld.global.nc.L1::no_allocate.v4.s32 {%0,%1,%2,%3}, [%4];"
+                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]) : "l"(p));
 }
 
 // Product type staged in shared memory: float products for a float matrix, double otherwise.
@@ -54,71 +56,87 @@ template <class Y>
 struct EpiStore {
     Y* y;
     struct Ops {};
-    __device__ __forceinline__ Ops load(int) const { return {}; }
+    __device__ __forceinline__ Ops load(int, int) const { return {}; }
     __device__ __forceinline__ void apply(int r, double s, const Ops&) const { y[r] = Y(s); }
 };
 
+// Epilogues: load(r, inst) fetches row r's operands before the matrix stream (inst = the row's instance in a
+// batch, 0 otherwise; step sizes par[2 inst] = tau, par[2 inst + 1] = sigma), apply(r, s, ops) consumes the sum.
 // Dual step of one row (gpu/pdhg.cu:178-190 semantics, running sum of z in FP64):
 //   v = z + sigma (2 s - Ax_old);  z = prox: v - sigma*rl if v/sigma < rl, v - sigma*ru if v/sigma > ru, else 0;
 //   Ax_old = s;  zs += z.
+// The arithmetic is FP64 whatever T is: with a small sigma, v - sigma*rl cancels, and in float that
+// cancellation stalls the method (the reference's --fp32 failure); only the stored values are rounded to T.
 template <class T>
 struct EpiRow {
     T *Ax, *z;
     double* zs;
-    const T *rl, *ru, *par;
-    struct Ops { T z, ax, rl, ru, sig; double zs; };
-    __device__ __forceinline__ Ops load(int r) const { return {z[r], Ax[r], rl[r], ru[r], par[1], zs[r]}; }
+    const T *rl, *ru;
+    const double* par;
+    struct Ops { double z, ax, rl, ru, sig, zs; };
+    __device__ __forceinline__ Ops load(int r, int inst) const {
+        return {double(z[r]), double(Ax[r]), double(rl[r]), double(ru[r]), par[2 * inst + 1], zs[r]};
+    }
     __device__ __forceinline__ void apply(int r, double s, const Ops& o) const {
-        T st = T(s), sig = o.sig;
-        T v = o.z + sig * (T(2) * st - o.ax), q = v / sig;
-        T zn = q < o.rl ? v - sig * o.rl : (q > o.ru ? v - sig * o.ru : T(0));
+        const T st = T(s);
+        const double sig = o.sig, v = o.z + sig * (2.0 * double(st) - o.ax), q = v / sig;
+        const T zn = T(q < o.rl ? v - sig * o.rl : (q > o.ru ? v - sig * o.ru : 0.0));
         Ax[r] = st, z[r] = zn, zs[r] = o.zs + double(zn);
     }
 };
 
 // Column step (gpu/pdhg.cu:192-206 semantics): ATz = s; with upd, the next primal step
-//   x = clamp(x - tau (c + s), l, u);  xs += x  (FP64 sum).
+//   x = clamp(x - tau (c + s), l, u);  xs += x  (FP64 arithmetic and sum, T storage).
 template <class T>
 struct EpiCol {
     T *ATz, *x;
     double* xs;
-    const T *c, *l, *u, *par;
+    const T *c, *l, *u;
+    const double* par;
     int upd;
-    struct Ops { T x, c, l, u, tau; double xs; };
-    __device__ __forceinline__ Ops load(int r) const {
-        if (!upd) return {T(0), T(0), T(0), T(0), T(0), 0.0};
-        return {x[r], c[r], l[r], u[r], par[0], xs[r]};
+    struct Ops { double x, c, l, u, tau, xs; };
+    __device__ __forceinline__ Ops load(int r, int inst) const {
+        if (!upd) return {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        return {double(x[r]), double(c[r]), double(l[r]), double(u[r]), par[2 * inst], xs[r]};
     }
     __device__ __forceinline__ void apply(int r, double s, const Ops& o) const {
-        T st = T(s);
+        const T st = T(s);
         ATz[r] = st;
         if (upd) {
-            T xn = clampv(o.x - o.tau * (o.c + st), o.l, o.u);
+            const T xn = T(clampv(o.x - o.tau * (o.c + double(st)), o.l, o.u));
             x[r] = xn, xs[r] = o.xs + double(xn);
         }
     }
 };
 
 // ------------------------------------------------------------------------------------------ SpMV skeleton
-// blk[b] = first row of block b (blk[nblk] = rows). VEC: the val/idx base pointers are 16-byte aligned.
-template <class T, class X, class E, bool VEC>
-__global__ void __launch_bounds__(kThreads) k_rowblock(const int* __restrict__ ptr, const int* __restrict__ idx,
-                                                         const T* __restrict__ val, const X* __restrict__ xin,
-                                                         const int* __restrict__ blk, const int* __restrict__ skip,
-                                                         E epi) {
-    using P = typename ProdT<T, X>::type;
-    __shared__ P prod[kTile];
-    __shared__ double rowsum[kRowsMax];
-    __shared__ int rptr[kRowsMax + 1];
-    if (skip && *skip) return;
-    const int b = blockIdx.x, tid = threadIdx.x;
-    const int r0 = blk[b], r1 = blk[b + 1], nrows = r1 - r0;
-    const int p0 = ptr[r0], p1 = ptr[r1], len = p1 - p0;
+// Row-block metadata, one int4 per block, built on the host (build_row_blocks): x = first row, y = number of rows,
+// z = first nonzero, w = end of the nonzeros. VEC: the val/idx base pointers are 16-byte aligned.
+constexpr int kShort = 48;                       // rows up to this length are summed by their own thread
+constexpr int kQuads = (kTile + 3 + 3) / 4 / kThreads;  // 16-byte quads per thread in the staging loop (2)
+static_assert(kQuads * 4 * kThreads >= kTile + 3, "a block's quads must fit the staging loop");
+__device__ __forceinline__ int pidx(int k) { return k + (k >> 5); }  // one pad slot per 32: no bank conflicts
 
-    typename E::Ops ops{};
-    const bool mine = tid < nrows;
-    if (mine) ops = epi.load(r0 + tid);
+template <class P>
+struct RowSmem {
+    P prod[kTile + kTile / 32];
+    double rowsum[kRowsMax];
+    int rptr[kRowsMax + 1];
+    short longrow[kRowsMax];
+    int nlong;
+};
 
+// Sums of the block's rows into sm.rowsum[0, nrows) (a long row: sm.rowsum[0]). Ends with a barrier.
+//   1. stage: each thread issues all of its 16-byte val / idx loads (up to kQuads quads), then all of its gathers
+//      of the vector entries, then writes the products to shared memory;
+//   2. reduce: a row of at most kShort nonzeros is summed sequentially by its own thread; longer rows are queued
+//      and each is summed by one warp (lanes strided, shuffle tree). Every row's summation order is fixed.
+template <class T, class X, bool VEC, class P>
+__device__ __forceinline__ void block_sums(const int* __restrict__ ptr, const int* __restrict__ idx,
+                                           const T* __restrict__ val, const X* __restrict__ xin, int4 meta,
+                                           RowSmem<P>& sm) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int r0 = meta.x, nrows = meta.y & 0xffff, p0 = meta.z, p1 = meta.w, len = p1 - p0;
     if (len > kTile) {  // one long row: strided partial sums, fixed-order block reduction
         double s = 0;
         if (VEC) {
@@ -138,68 +156,127 @@ __global__ void __launch_bounds__(kThreads) k_rowblock(const int* __restrict__ p
             for (int k = p0 + tid; k < p1; k += kThreads) s += double(__ldg(val + k)) * double(__ldg(xin + __ldg(idx + k)));
         }
         for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
-        if ((tid & 31) == 0) rowsum[tid >> 5] = s;
+        if (lane == 0) sm.rowsum[1 + warp] = s;
         __syncthreads();
         if (tid == 0) {
             double t = 0;
-            for (int w = 0; w < kThreads / 32; ++w) t += rowsum[w];
-            epi.apply(r0, t, ops);
+            for (int w = 0; w < kThreads / 32; ++w) t += sm.rowsum[1 + w];
+            sm.rowsum[0] = t;
         }
+        __syncthreads();
         return;
     }
 
     // 1. stage products
-    for (int t = tid; t <= nrows; t += kThreads) rptr[t] = ptr[r0 + t] - p0;
+    for (int t = tid; t <= nrows; t += kThreads) sm.rptr[t] = ptr[r0 + t] - p0;
+    if (tid == 0) sm.nlong = 0;
     if (VEC) {
         const int a0 = p0 & ~3;
-        for (int q = a0 + 4 * tid; q < p1; q += 4 * kThreads) {
+        T v[kQuads][4];
+        int c[kQuads][4];
+#pragma unroll
+        for (int i = 0; i < kQuads; ++i) {
+            const int q = a0 + 4 * (tid + i * kThreads);
             if (q >= p0 && q + 4 <= p1) {
-                T v[4]; int c[4];
-                Quad<T>::load(val + q, v), load_idx4(idx + q, c);
-                X g[4];
-#pragma unroll
-                for (int e = 0; e < 4; ++e) g[e] = __ldg(xin + c[e]);
-#pragma unroll
-                for (int e = 0; e < 4; ++e) prod[q - p0 + e] = P(v[e]) * P(g[e]);
+                Quad<T>::load(val + q, v[i]), load_idx4(idx + q, c[i]);
             } else {
+#pragma unroll
                 for (int e = 0; e < 4; ++e) {
-                    int k = q + e;
-                    if (k >= p0 && k < p1) prod[k - p0] = P(__ldg(val + k)) * P(__ldg(xin + __ldg(idx + k)));
+                    const bool in = q + e >= p0 && q + e < p1;
+                    v[i][e] = in ? __ldg(val + q + e) : T(0);
+                    c[i][e] = in ? __ldg(idx + q + e) : -1;
                 }
             }
         }
+        X g[kQuads][4];
+#pragma unroll
+        for (int i = 0; i < kQuads; ++i)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) g[i][e] = c[i][e] >= 0 ? __ldg(xin + c[i][e]) : X(0);
+#pragma unroll
+        for (int i = 0; i < kQuads; ++i) {
+            const int q = a0 + 4 * (tid + i * kThreads);
+#pragma unroll
+            for (int e = 0; e < 4; ++e)
+                if (c[i][e] >= 0) sm.prod[pidx(q + e - p0)] = P(v[i][e]) * P(g[i][e]);
+        }
     } else {
-        for (int k = p0 + tid; k < p1; k += kThreads) prod[k - p0] = P(__ldg(val + k)) * P(__ldg(xin + __ldg(idx + k)));
+        for (int k = p0 + tid; k < p1; k += kThreads) sm.prod[pidx(k - p0)] = P(__ldg(val + k)) * P(__ldg(xin + __ldg(idx + k)));
     }
     __syncthreads();
 
-    // 2. reduce rows with G-lane groups
-    int mean = nrows > 0 ? (len + nrows - 1) / nrows : 1;
-    int G = 1;
-    while (G < 32 && G < mean) G <<= 1;
-    const int lane = tid & (G - 1), grp = tid / G, ngrp = kThreads / G;
-    for (int base = 0; base < nrows; base += ngrp) {  // CTA-uniform trip count: every lane reaches the shuffles
-        const int t = base + grp;
+    // 2. reduce: short rows by their own thread, long rows by a warp each
+    if (tid < nrows) {
+        const int a = sm.rptr[tid], b = sm.rptr[tid + 1];
+        if (b - a <= kShort) {
+            double s = 0;
+            for (int k = a; k < b; ++k) s += double(sm.prod[pidx(k)]);
+            sm.rowsum[tid] = s;
+        } else {
+            sm.longrow[atomicAdd(&sm.nlong, 1)] = short(tid);
+        }
+    }
+    __syncthreads();
+    for (int i = warp; i < sm.nlong; i += kThreads / 32) {  // warp-uniform trip count: all lanes shuffle
+        const int t = sm.longrow[i];
         double s = 0;
-        if (t < nrows)
-            for (int k = rptr[t] + lane; k < rptr[t + 1]; k += G) s += double(prod[k]);
-        for (int off = G >> 1; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off, G);
-        if (t < nrows && lane == 0) rowsum[t] = s;
+        for (int k = sm.rptr[t] + lane; k < sm.rptr[t + 1]; k += 32) s += double(sm.prod[pidx(k)]);
+        for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+        if (lane == 0) sm.rowsum[t] = s;
     }
     __syncthreads();
+}
 
-    // 3. epilogue
-    if (mine) epi.apply(r0 + tid, rowsum[tid], ops);
+// One launch over all row blocks of one matrix; `skip` (may be NULL): return at once when *skip != 0.
+template <class T, class X, class E, bool VEC>
+__global__ void __launch_bounds__(kThreads) k_rowblock(const int* __restrict__ ptr, const int* __restrict__ idx,
+                                                         const T* __restrict__ val, const X* __restrict__ xin,
+                                                         const int4* __restrict__ blk, const int* __restrict__ skip,
+                                                         E epi) {
+    using P = typename ProdT<T, X>::type;
+    __shared__ RowSmem<P> sm;
+    if (skip && *skip) return;
+    const int tid = threadIdx.x;
+    const int4 meta = __ldg(blk + blockIdx.x);
+    const int r0 = meta.x, nrows = meta.y & 0xffff;
+    typename E::Ops ops{};
+    const bool mine = tid < nrows;
+    if (mine) ops = epi.load(r0 + tid, 0);
+    block_sums<T, X, VEC>(ptr, idx, val, xin, meta, sm);
+    if (mine) epi.apply(r0 + tid, sm.rowsum[tid], ops);
+}
+
+// Batched form: a block list over many instances (block-diagonal batch). ext[b] = {instance, row shift, gather
+// offset, 0}: the block's rows r of the (possibly shared) matrix are rows r + shift of the concatenated instance
+// vectors, and its column indices address xin + offset. Blocks of instances with active[instance] == 0 return.
+template <class T, class X, class E, bool VEC>
+__global__ void __launch_bounds__(kThreads) k_rowblock_batch(const int* __restrict__ ptr, const int* __restrict__ idx,
+                                                               const T* __restrict__ val, const X* __restrict__ xin,
+                                                               const int4* __restrict__ blk,
+                                                               const int4* __restrict__ ext,
+                                                               const int* __restrict__ active, E epi) {
+    using P = typename ProdT<T, X>::type;
+    __shared__ RowSmem<P> sm;
+    const int4 e4 = __ldg(ext + blockIdx.x);
+    if (!active[e4.x]) return;
+    const int tid = threadIdx.x;
+    const int4 meta = __ldg(blk + blockIdx.x);
+    const int r0 = meta.x + e4.y, nrows = meta.y & 0xffff;
+    typename E::Ops ops{};
+    const bool mine = tid < nrows;
+    if (mine) ops = epi.load(r0 + tid, e4.x);
+    block_sums<T, X, VEC>(ptr, idx, val, xin + e4.z, meta, sm);
+    if (mine) epi.apply(r0 + tid, sm.rowsum[tid], ops);
 }
 
 // First primal step of a block (gpu/pdhg.cu:208-214): x = clamp(x - tau (c + ATz), l, u), xs += x.
 template <class T>
 __global__ void k_xupd(int n, T* __restrict__ x, const T* __restrict__ ATz, const T* __restrict__ c,
-                       const T* __restrict__ l, const T* __restrict__ u, const T* __restrict__ par,
+                       const T* __restrict__ l, const T* __restrict__ u, const double* __restrict__ par,
                        double* __restrict__ xs) {
-    const T tau = par[0];
+    const double tau = par[0];
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
-        T xn = clampv(x[j] - tau * (c[j] + ATz[j]), l[j], u[j]);
+        const T xn = T(clampv(double(x[j]) - tau * (double(c[j]) + double(ATz[j])), double(l[j]), double(u[j])));
         x[j] = xn, xs[j] += double(xn);
     }
 }
@@ -304,7 +381,7 @@ __global__ void __launch_bounds__(kRedThreads) k_power_sumsq(int n, const T* __r
     reduce_finish<1>(a, part, ticket, out);
 }
 
-__global__ void k_power_update(const double* out, double* st, int* done, int it) {  // one thread
+static __global__ void k_power_update(const double* out, double* st, int* done, int it) {  // one thread
     if (*done) return;
     double s = out[0], prev = st[0];
     if (s <= 0) { st[0] = 0, *done = 1; return; }
@@ -320,8 +397,7 @@ __global__ void k_power_scale(int n, T* __restrict__ v, const double* __restrict
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) v[j] = T(double(v[j]) * f);
 }
 
-template <class T>
-__global__ void k_set_par(T* par, T tau, T sigma) { par[0] = tau, par[1] = sigma; }
+static __global__ void k_set_par(double* par, double tau, double sigma) { par[0] = tau, par[1] = sigma; }
 
 // Default start (gpu/pdhg.cu:450-455): x = x_last = clamp(0, l, u), sum <- 0.
 template <class T>

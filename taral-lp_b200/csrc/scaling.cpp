@@ -24,15 +24,13 @@ Csr transpose(const Csr& a, int cols) {  // counting sort; rows of the output as
     return t;
 }
 
-Scaled build_scaled(const taral_model& md, double sign) {
-    Scaled P;
+void scale_matrix(const taral_model& md, Scaled& P) {
     P.n = md.n, P.m = md.m;
     Csr T;  // A^T from the column-wise model, zero entries dropped
     T.rows = P.n;
     T.ptr.assign(size_t(P.n) + 1, 0);
-    const int64_t base = md.col_ptr[0];
-    T.idx.reserve(size_t(md.col_ptr[P.n] - base));
-    T.val.reserve(size_t(md.col_ptr[P.n] - base));
+    T.idx.reserve(size_t(md.col_ptr[P.n] - md.col_ptr[0]));
+    T.val.reserve(size_t(md.col_ptr[P.n] - md.col_ptr[0]));
     for (int j = 0; j < P.n; ++j) {
         for (int64_t k = md.col_ptr[j]; k < md.col_ptr[j + 1]; ++k)
             if (md.val[k] != 0) T.idx.push_back(md.row_idx[k]), T.val.push_back(md.val[k]);
@@ -72,12 +70,18 @@ Scaled build_scaled(const taral_model& md, double sign) {
         for (int64_t k = A.ptr[i]; k < A.ptr[i + 1]; ++k) rs[i] += std::fabs(A.val[k]), cs[A.idx[k]] += std::fabs(A.val[k]);
     apply();
     P.AT = transpose(A, P.n);
+}
+
+void scale_vectors(const taral_model& md, double sign, const std::vector<double>& Dr, const std::vector<double>& Dc,
+                   Scaled& P) {
+    P.m = md.m, P.n = md.n;
     P.c.resize(size_t(P.n)), P.l.resize(size_t(P.n)), P.u.resize(size_t(P.n));
     P.rl.resize(size_t(P.m)), P.ru.resize(size_t(P.m));
+    P.cnorm = P.bnorm = 0;
     for (int j = 0; j < P.n; ++j) {
         double c = sign * md.cost[j];
         P.cnorm += c * c;
-        P.c[j] = c * P.Dc[j], P.l[j] = md.col_lo[j] / P.Dc[j], P.u[j] = md.col_up[j] / P.Dc[j];
+        P.c[j] = c * Dc[j], P.l[j] = md.col_lo[j] / Dc[j], P.u[j] = md.col_up[j] / Dc[j];
     }
     for (int i = 0; i < P.m; ++i) {
         double lo = md.row_lo[i], up = md.row_up[i], b = 0;
@@ -85,9 +89,15 @@ Scaled build_scaled(const taral_model& md, double sign) {
         else if (std::isfinite(lo)) b = std::fabs(lo);
         else if (std::isfinite(up)) b = std::fabs(up);
         P.bnorm += b * b;
-        P.rl[i] = lo * P.Dr[i], P.ru[i] = up * P.Dr[i];
+        P.rl[i] = lo * Dr[i], P.ru[i] = up * Dr[i];
     }
     P.bnorm = std::sqrt(P.bnorm), P.cnorm = std::sqrt(P.cnorm);
+}
+
+Scaled build_scaled(const taral_model& md, double sign) {
+    Scaled P;
+    scale_matrix(md, P);
+    scale_vectors(md, sign, P.Dr, P.Dc, P);
     return P;
 }
 

@@ -98,7 +98,7 @@ int solve_model(const taral_model& md, const Options& o, SolveResult& res, const
     double setup = res.scale_s + res.device_init_s + res.transfer_s;
     t = Clock::now();
     try {
-        res.outcome = run(*e, P, o, o.time_limit - setup, x0_orig ? xs0.data() : nullptr,
+        res.outcome = run(*e, DriverData::of(P), o, o.time_limit - setup, x0_orig ? xs0.data() : nullptr,
                           y0_orig ? zs0.data() : nullptr);
     } catch (const std::exception& ex) {
         res.error = ex.what();
@@ -162,6 +162,28 @@ extern "C" int taral_pdhg_solve(const taral_model* md, const taral_options* o, t
 extern "C" int taral_pdhg_solve_warm(const taral_model* md, const taral_options* o, const double* x0,
                                      const double* y0, taral_outcome* out, double* x_out, double* y_out) {
     return solve_c(md, o, out, x_out, y_out, x0, y0);
+}
+
+extern "C" int pdhg_create_model(const taral_model* md, int precision, int eval_freq, unsigned flags, pdhg_ctx** out,
+                                 double* bnorm, double* cnorm) {
+    if (!md || !out) return TARAL_ERR_INPUT;
+    *out = nullptr;
+    if (taral::input_error(*md)) return TARAL_ERR_UNSUPPORTED;
+    if (!taral::check_model(*md).empty()) return TARAL_ERR_INPUT;
+    taral::Scaled P;
+    try {
+        P = taral::build_scaled(*md, md->maximize ? -1.0 : 1.0);
+    } catch (const std::bad_alloc&) {
+        return TARAL_ERR_ALLOC;
+    }
+    taral_csr A = P.A.view(P.n), AT = P.AT.view(P.m);
+    int rc = pdhg_create(&A, &AT, P.c.data(), P.l.data(), P.u.data(), P.rl.data(), P.ru.data(), P.Dr.data(),
+                         P.Dc.data(), P.m, P.n, precision, eval_freq, flags, out);
+    if (rc == TARAL_OK) {
+        if (bnorm) *bnorm = P.bnorm;
+        if (cnorm) *cnorm = P.cnorm;
+    }
+    return rc;
 }
 
 // ------------------------------------------------------------------------------------------------ MPS handle

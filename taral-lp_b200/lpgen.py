@@ -341,3 +341,121 @@ def general(m: int, n: int, per_col: int = 4, seed: int = 0, maximize: bool = Fa
         c = -c
     return LP(name=f"GENERAL_{m}x{n}_{seed}", m=m, n=n, col_ptr=col_ptr, row_idx=ri, val=v, cost=c,
               col_lo=lo, col_up=up, row_lo=rlo, row_up=rup, obj_const=0.5, maximize=maximize, row_types=types)
+
+
+# ---------------------------------------------------------------------------------------------- refinery family
+# One period block: 1,500 rows x 4,000 columns.
+#   columns  [0,1000) process (crude -> unit) activities   [1000,3000) intermediate flows to blend pools
+#            [3000,3800) product sales                       [3800,4000) closing inventory of 200 storable items
+#   rows     [0,500) yield balances (E)   [500,800) unit capacities (L)   [800,1300) blend quality (G)
+#            [1300,1500) inventory balances (E)
+# A process column yields into 26 intermediates with U(0,1) coefficients scaled to sum U(0.85,1) (<= 1) and uses
+# 3 capacity rows (coefficient 1). A flow column consumes its intermediate (-1) and carries U(-1,1) quality
+# coefficients into 12 quality rows; 10% also feed an inventory balance (+1). A sales column has U(-1,1) in 18
+# quality rows and draws -1 from an inventory balance. An inventory column is -1 in its item's balance of period
+# t and +1 in that of period t+1 (the linking rows). About 71k nonzeros per period (3.4M at 48 periods).
+# Bounds 0 <= x <= U(100,1000) (capacities), costs U(-50,50) (prices). A point x0 in [0, 0.5 x capacity] is
+# planted: yield and inventory rows are equalities at A x0, capacity rows allow 1.3 A x0 + 10, quality rows
+# require at least A x0 - U(0,1)(1 + |A x0|). Perturbation: 128 price groups scale costs and 128 capacity groups
+# scale column capacities and capacity-row limits, each by a factor in [0.8, 1.2]; x0 stays feasible.
+REF_ROWS, REF_COLS, REF_GROUPS = 1500, 4000, 128
+
+
+class RefineryBase:
+    """The 48-period structure of one scenario family (matrix, planted point, base prices and capacities)."""
+
+    def __init__(self, periods: int = 48, seed: int = 7):
+        rng = np.random.default_rng(seed)
+        R, Cn = REF_ROWS, REF_COLS
+        self.periods, self.seed = periods, seed
+        rows_l, cols_l, vals_l = [], [], []
+        for t in range(periods):
+            r0, c0 = t * R, t * Cn
+            # process columns
+            nP = 1000
+            yr = np.sort(np.stack([rng.choice(500, 26, replace=False) for _ in range(nP)]), axis=1)
+            yv = rng.uniform(0, 1, (nP, 26))
+            yv *= (rng.uniform(0.85, 1.0, nP) / yv.sum(axis=1))[:, None]
+            cr = np.sort(np.stack([rng.choice(300, 3, replace=False) for _ in range(nP)]), axis=1) + 500
+            pc = np.repeat(np.arange(nP), 29)
+            rows_l.append(r0 + np.concatenate([yr, cr], axis=1).ravel())
+            cols_l.append(c0 + pc)
+            vals_l.append(np.concatenate([yv, np.ones((nP, 3))], axis=1).ravel())
+            # flow columns
+            nF = 2000
+            src = rng.integers(0, 500, nF)
+            qr = np.stack([rng.choice(500, 12, replace=False) for _ in range(nF)]) + 800
+            qv = rng.uniform(-1, 1, (nF, 12))
+            inv = rng.random(nF) < 0.1
+            invr = rng.integers(0, 200, nF) + 1300
+            for_rows = [src, qr]
+            fr = np.concatenate([src[:, None], qr], axis=1)
+            fv = np.concatenate([-np.ones((nF, 1)), qv], axis=1)
+            fc = np.repeat(np.arange(1000, 1000 + nF), 13)
+            rows_l.append(r0 + fr.ravel()), cols_l.append(c0 + fc), vals_l.append(fv.ravel())
+            rows_l.append(r0 + invr[inv]), cols_l.append(c0 + 1000 + np.nonzero(inv)[0]), vals_l.append(np.ones(inv.sum()))
+            # sales columns
+            nS = 800
+            sr = np.stack([rng.choice(500, 18, replace=False) for _ in range(nS)]) + 800
+            sv = rng.uniform(-1, 1, (nS, 18))
+            sb = rng.integers(0, 200, nS) + 1300
+            rows_l.append(r0 + np.concatenate([sr, sb[:, None]], axis=1).ravel())
+            cols_l.append(c0 + np.repeat(np.arange(3000, 3000 + nS), 19))
+            vals_l.append(np.concatenate([sv, -np.ones((nS, 1))], axis=1).ravel())
+            # inventory columns: -1 in this period's balance, +1 in the next period's
+            k = np.arange(200)
+            rows_l.append(r0 + 1300 + k), cols_l.append(c0 + 3800 + k), vals_l.append(-np.ones(200))
+            if t + 1 < periods:
+                rows_l.append(r0 + R + 1300 + k), cols_l.append(c0 + 3800 + k), vals_l.append(np.ones(200))
+        rows = np.concatenate(rows_l).astype(np.int64)
+        cols = np.concatenate(cols_l).astype(np.int64)
+        vals = _r12(np.concatenate(vals_l))
+        order = np.lexsort((rows, cols))
+        self.rows, self.cols, self.vals = rows[order].astype(np.int32), cols[order], vals[order]
+        self.m, self.n = periods * R, periods * Cn
+        self.cap = np.round(rng.uniform(100, 1000, self.n), 3)
+        self.price = np.round(rng.uniform(-50, 50, self.n), 4)
+        self.x0 = rng.uniform(0, 0.5, self.n) * self.cap
+        self.qslack = rng.uniform(0, 1, self.m)
+        self.price_group = np.tile(rng.integers(0, REF_GROUPS, Cn), periods)
+        self.cap_group_col = np.tile(rng.integers(0, REF_GROUPS, Cn), periods)
+        self.cap_group_row = np.tile(rng.integers(0, REF_GROUPS, R), periods)
+
+    def instance(self, periods: int, perturb: Optional[np.ndarray] = None, name: Optional[str] = None) -> LP:
+        """The LP of the first `periods` periods, with prices / capacities scaled by the 256-vector `perturb`
+        (None: all ones). The links of the last period to a later one are dropped."""
+        R, Cn = REF_ROWS, REF_COLS
+        m, n = periods * R, periods * Cn
+        keep = (self.cols < n) & (self.rows < m)
+        cols, rows, vals = self.cols[keep], self.rows[keep], self.vals[keep]
+        col_ptr = np.zeros(n + 1, np.int64)
+        np.cumsum(np.bincount(cols, minlength=n), out=col_ptr[1:])
+        p = np.ones(2 * REF_GROUPS) if perturb is None else np.asarray(perturb, np.float64)
+        fprice = p[self.price_group[:n]]
+        fcap_c = p[REF_GROUPS + self.cap_group_col[:n]]
+        fcap_r = p[REF_GROUPS + self.cap_group_row[:m]]
+        x0 = self.x0[:n]
+        ax0 = np.zeros(m)
+        np.add.at(ax0, rows, vals * x0[cols])
+        rtype = np.empty(m, np.int8)
+        loc = np.arange(m) % R
+        rtype[loc < 500] = 0                      # E yield
+        rtype[(loc >= 500) & (loc < 800)] = 1     # L capacity
+        rtype[(loc >= 800) & (loc < 1300)] = 2    # G quality
+        rtype[loc >= 1300] = 0                    # E inventory
+        row_lo = np.where(rtype == 0, ax0, np.where(rtype == 2, ax0 - self.qslack[:m] * (1 + np.abs(ax0)), -INF))
+        row_up = np.where(rtype == 0, ax0, np.where(rtype == 1, (1.3 * ax0 + 10) * fcap_r, INF))
+        return LP(name=name or f"REFINERY_T{periods}", m=m, n=n, col_ptr=col_ptr, row_idx=rows, val=vals,
+                  cost=_r12(self.price[:n] * fprice), col_lo=np.zeros(n), col_up=_r12(self.cap[:n] * fcap_c),
+                  row_lo=_r12(row_lo), row_up=_r12(row_up),
+                  row_types=["E" if k == 0 else ("L" if k == 1 else "G") for k in rtype], x_star=x0)
+
+
+def refinery(periods: int = 48, seed: int = 7, perturb: Optional[np.ndarray] = None) -> LP:
+    """Refinery-structured multi-period LP (48 periods: 72,000 rows x 192,000 columns, ~3.4M nonzeros)."""
+    return RefineryBase(max(periods, 1), seed).instance(periods, perturb)
+
+
+def perturbations(count: int, seed: int) -> np.ndarray:
+    """`count` independent 256-vectors of price / capacity factors, U(0.8, 1.2)."""
+    return np.random.default_rng(seed).uniform(0.8, 1.2, (count, 2 * REF_GROUPS))

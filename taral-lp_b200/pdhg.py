@@ -62,7 +62,7 @@ class OutcomeT(C.Structure):
                 ("max_row_violation", C.c_double), ("max_bound_violation", C.c_double), ("scale_s", C.c_double),
                 ("device_init_s", C.c_double), ("transfer_s", C.c_double), ("solve_s", C.c_double),
                 ("power_iter_s", C.c_double), ("device_mem_bytes", C.c_size_t), ("kernel_launches", C.c_int64),
-                ("nnz", C.c_int64)]
+                ("nnz", C.c_int64), ("device_s", C.c_double)]
 
 
 # Every symbol the header declares, with its ctypes signature: (restype, argtypes).
@@ -78,6 +78,9 @@ SIGNATURES = {
     "pdhg_restart": (C.c_int, [C.c_void_p, C.c_int, C.c_double]),
     "pdhg_download": (C.c_int, [C.c_void_p, C.c_int, C.c_double, _dp, _dp]),
     "pdhg_info": (C.c_int, [C.c_void_p, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]),
+    "pdhg_create_model": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_uint, C.POINTER(C.c_void_p), _dp, _dp]),
+    "pdhg_solve_ctx": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_void_p, _dp, _dp, C.c_void_p, _dp, _dp]),
+    "pdhg_profile_phases": (C.c_int, [C.c_void_p, C.c_int, _dp, _dp]),
     "pdhg_kernel_launches": (C.c_int64, [C.c_void_p]),
     "pdhg_last_error": (C.c_char_p, [C.c_void_p]),
     "pdhg_destroy": (None, [C.c_void_p]),
@@ -93,6 +96,12 @@ SIGNATURES = {
     "taral_mps_row_name": (C.c_char_p, [C.c_void_p, C.c_int]),
     "taral_mps_name": (C.c_char_p, [C.c_void_p]),
     "taral_mps_free": (None, [C.c_void_p]),
+    "taral_batch_create": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(OptionsT), C.POINTER(C.c_void_p)]),
+    "taral_batch_solve": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "taral_batch_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_size_t), C.POINTER(C.c_int64),
+                                   C.POINTER(C.c_int64)]),
+    "taral_batch_last_error": (C.c_char_p, [C.c_void_p]),
+    "taral_batch_destroy": (None, [C.c_void_p]),
     "taral_spmv_plan_create": (C.c_int, [C.c_int, C.c_int, _lp, C.c_int, C.POINTER(C.c_void_p)]),
     "taral_spmv_run": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                  C.c_void_p]),
@@ -172,6 +181,18 @@ class Engine:
         self.h = h
 
     @classmethod
+    def from_model(cls, lp, precision=FP64, eval_freq=64, graph=True):
+        """Scale a column-wise model on the host (gpu/pdhg.cu:80-133) and upload it. Sets .bnorm / .cnorm."""
+        mr = _Model(lp)
+        h = C.c_void_p()
+        bn, cn = C.c_double(), C.c_double()
+        _check(lib().pdhg_create_model(C.byref(mr.s), int(precision), int(eval_freq), 0 if graph else 1, C.byref(h),
+                                       C.byref(bn), C.byref(cn)))
+        self = cls.__new__(cls)
+        self.h, self.m, self.n, self.bnorm, self.cnorm = h, int(lp.m), int(lp.n), bn.value, cn.value
+        return self
+
+    @classmethod
     def from_scaled(cls, sp, **kw):
         """From an object with A, AT (ptr, idx, val) tuples and c, l, u, rl, ru, Dr, Dc arrays."""
         return cls(sp.A, sp.AT, sp.c, sp.l, sp.u, sp.rl, sp.ru, sp.Dr, sp.Dc, **kw)
@@ -209,6 +230,28 @@ class Engine:
         x, z = np.zeros(max(self.n, 1)), np.zeros(max(self.m, 1))
         _check(lib().pdhg_download(self.h, int(avg), float(f), _p(x), _p(z)), self.h)
         return x[:self.n], z[:self.m]
+
+    def solve(self, bnorm, cnorm, tol=1e-4, time_limit=3600.0, max_iter=2_000_000_000, eval_freq=64, row_rel=0.0,
+              x0=None, z0=None, want_point=True):
+        """The reference driver (gpu/pdhg.cu:761-849) on this context. Returns (outcome dict, x, z) in the scaled
+        space; outcome['device_s'] is the CUDA-event time of the solve."""
+        o = OptionsT(tol, time_limit, max_iter, eval_freq, row_rel, 0, 1, 0)
+        r = OutcomeT()
+        x, z = (np.zeros(max(self.n, 1)), np.zeros(max(self.m, 1))) if want_point else (None, None)
+        xa = None if x0 is None else _f64(x0)
+        za = None if z0 is None else _f64(z0)
+        _check(lib().pdhg_solve_ctx(self.h, float(bnorm), float(cnorm), C.byref(o), None if xa is None else _p(xa),
+                                    None if za is None else _p(za), C.byref(r), None if x is None else _p(x),
+                                    None if z is None else _p(z)), self.h)
+        out = {k: getattr(r, k) for k, _ in OutcomeT._fields_}
+        out["status"] = STATUS[r.status]
+        return out, (None if x is None else x[:self.n]), (None if z is None else z[:self.m])
+
+    def profile_phases(self, reps):
+        """Mean CUDA-event milliseconds per launch of the row-phase and column-phase kernels over `reps` steps."""
+        a, b = C.c_double(), C.c_double()
+        _check(lib().pdhg_profile_phases(self.h, int(reps), C.byref(a), C.byref(b)), self.h)
+        return a.value, b.value
 
     def info(self):
         buf = C.create_string_buffer(256)
@@ -264,6 +307,69 @@ def solve(lp, tol=1e-4, time_limit=3600.0, max_iter=2_000_000_000, eval_freq=64,
     out = {k: getattr(r, k) for k, _ in OutcomeT._fields_}
     out["status"] = STATUS[r.status]
     return out, x[:lp.n], y[:lp.m]
+
+
+# ------------------------------------------------------------------------------------------------ batch
+class Batch:
+    """Many LPs solved together (taral_batch_*): per-instance restarts and stopping on the device, identical
+    constraint matrices stored once. Keeps the models' arrays alive for the batch's lifetime."""
+
+    def __init__(self, lps, tol=1e-4, time_limit=3600.0, max_iter=2_000_000_000, eval_freq=64, row_rel=0.0,
+                 precision=FP64, graph=True):
+        self.lps = list(lps)
+        self._models = [_Model(lp) for lp in self.lps]
+        arr = (ModelT * len(self._models))(*[m.s for m in self._models])
+        self._arr = arr
+        o = OptionsT(tol, time_limit, max_iter, eval_freq, row_rel, 0, int(graph), int(precision))
+        h = C.c_void_p()
+        _check(lib().taral_batch_create(C.cast(arr, C.c_void_p), len(self._models), C.byref(o), C.byref(h)))
+        self.h = h
+
+    def info(self):
+        d, mem, ns, nt = C.c_int(), C.c_size_t(), C.c_int64(), C.c_int64()
+        _check(lib().taral_batch_info(self.h, C.byref(d), C.byref(mem), C.byref(ns), C.byref(nt)))
+        return {"distinct_matrices": d.value, "device_mem_bytes": mem.value, "nnz_stored": ns.value,
+                "nnz_total": nt.value}
+
+    def solve(self, x0=None, y0=None, want_points=True):
+        """Returns (list of outcome dicts, list of x, list of y). x0 / y0: optional lists of warm starts (entries
+        may be None)."""
+        k = len(self.lps)
+        outs = (OutcomeT * k)()
+
+        def table(arrs):  # array of double* (NULL where None), as a void*
+            if arrs is None:
+                return None, None
+            t = (_dp * k)(*[None if a is None else _p(a) for a in arrs])
+            return t, C.cast(t, C.c_void_p)
+        xin = None if x0 is None else [None if v is None else _f64(v) for v in x0]
+        yin = None if y0 is None else [None if v is None else _f64(v) for v in y0]
+        xout = [np.zeros(max(lp.n, 1)) for lp in self.lps] if want_points else None
+        yout = [np.zeros(max(lp.m, 1)) for lp in self.lps] if want_points else None
+        tabs = [table(v) for v in (xin, yin, xout, yout)]
+        code = lib().taral_batch_solve(self.h, tabs[0][1], tabs[1][1], C.cast(outs, C.c_void_p), tabs[2][1],
+                                       tabs[3][1])
+        if code != OK:
+            raise TaralError(code, (lib().taral_batch_last_error(self.h) or b"").decode())
+        res = []
+        for i in range(k):
+            d = {f: getattr(outs[i], f) for f, _ in OutcomeT._fields_}
+            d["status"] = STATUS[outs[i].status]
+            res.append(d)
+        if not want_points:
+            return res, None, None
+        return res, [xout[i][:self.lps[i].n] for i in range(k)], [yout[i][:self.lps[i].m] for i in range(k)]
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().taral_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 # ------------------------------------------------------------------------------------------------ MPS

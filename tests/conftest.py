@@ -55,3 +55,21 @@ def golden(name):
 
 def rel(a, b):
     return abs(a - b) / max(1.0, abs(b))
+
+
+class _BoundedPdhg:
+    """The pdhg binding with a 120 s default time limit on whole solves, so a regression fails instead of
+    running to the engine's 3600 s default."""
+
+    def __getattr__(self, name):
+        import pdhg
+        return getattr(pdhg, name)
+
+    @staticmethod
+    def solve(lp, **kw):
+        import pdhg
+        kw.setdefault("time_limit", 120.0)
+        return pdhg.solve(lp, **kw)
+
+
+bounded_pdhg = _BoundedPdhg()

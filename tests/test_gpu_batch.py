@@ -1,0 +1,72 @@
+"""Batched solves (taral_batch_*) against single-instance solves of the same models.
+
+Each instance follows the reference driver's rules with its own restarts and stopping, evaluated on the device.
+The batch sums its KKT scalars per row block and evaluates the restart rule in device FP64, so its arithmetic
+matches the single-instance path to rounding: statuses agree, iteration counts agree to within one evaluation
+block in FP64, objectives to 1e-7 relative."""
+import numpy as np
+import pytest
+
+import lpgen
+from conftest import bounded_pdhg as pdhg, rel
+
+pytestmark = pytest.mark.gpu
+
+
+def _single(lp, **kw):
+    r, x, y = pdhg.solve(lp, **kw)
+    return r
+
+
+def test_batch_of_distinct_models_fp64(engine_lib):
+    lps = [lpgen.general(120 + 20 * k, 300 + 30 * k, seed=k) for k in range(6)] + [lpgen.packing(1500, seed=4),
+                                                                                  lpgen.transport(12, 17, seed=5)]
+    b = pdhg.Batch(lps, tol=1e-6, time_limit=120)
+    assert b.info()["distinct_matrices"] == len(lps)
+    res, xs, ys = b.solve()
+    for lp, r, x in zip(lps, res, xs):
+        s = _single(lp, tol=1e-6)
+        assert r["status"] == s["status"] == "near_optimal", (lp.name, r, s)
+        assert abs(r["iterations"] - s["iterations"]) <= 64, (lp.name, r["iterations"], s["iterations"])
+        assert rel(r["objective"], s["objective"]) < 1e-7, (lp.name, r["objective"], s["objective"])
+        assert max(r["rel_primal"], r["rel_dual"], r["rel_gap"]) <= 1e-6
+        assert len(x) == lp.n
+
+
+def test_batch_shares_matrices_fp32(engine_lib):
+    base = lpgen.RefineryBase(3, seed=11)
+    pert = lpgen.perturbations(5, seed=2)
+    lps = [base.instance(2, pert[0]), base.instance(3, pert[1]), base.instance(2, pert[2]), base.instance(3, pert[3]),
+           base.instance(2, pert[4])]
+    b = pdhg.Batch(lps, tol=1e-6, precision=pdhg.FP32, time_limit=300)
+    info = b.info()
+    assert info["distinct_matrices"] == 2 and info["nnz_stored"] < info["nnz_total"]
+    res, xs, ys = b.solve()
+    for lp, r in zip(lps, res):
+        assert r["status"] == "near_optimal", (lp.name, r)
+        s = _single(lp, tol=1e-6)
+        assert rel(r["objective"], s["objective"]) < 5e-6, (lp.name, r["objective"], s["objective"])
+
+
+def test_batch_warm_start_and_limits(engine_lib):
+    lps = [lpgen.general(150, 350, seed=k) for k in range(3)]
+    b = pdhg.Batch(lps, tol=1e-6, time_limit=120)
+    res, xs, ys = b.solve()
+    res2, _, _ = b.solve(x0=xs, y0=ys)  # warm start from the answers: a few blocks at most
+    for r, r2 in zip(res, res2):
+        assert r2["status"] == "near_optimal" and r2["iterations"] < r["iterations"] / 4
+    res3, _, _ = b.solve(x0=[xs[0], None, None], y0=[ys[0], None, None])  # only instance 0 warm
+    assert res3[0]["iterations"] < res[0]["iterations"] / 4
+    assert [r["iterations"] for r in res3[1:]] == [r["iterations"] for r in res[1:]]
+    b2 = pdhg.Batch(lps, tol=1e-12, max_iter=128, time_limit=120)
+    res4, _, _ = b2.solve()
+    assert all(r["status"] == "iteration_limit" and r["iterations"] == 128 for r in res4)
+
+
+def test_batch_deterministic(engine_lib):
+    lps = [lpgen.general(100, 260, seed=k) for k in range(4)]
+    b = pdhg.Batch(lps, tol=1e-6, time_limit=120)
+    r1, x1, _ = b.solve()
+    r2, x2, _ = b.solve()
+    assert [r["iterations"] for r in r1] == [r["iterations"] for r in r2]
+    assert all(np.array_equal(a, c) for a, c in zip(x1, x2))

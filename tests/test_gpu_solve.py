@@ -12,7 +12,8 @@ import pytest
 
 import lpgen
 import oracle
-import pdhg
+import pdhg as _pdhg
+from conftest import bounded_pdhg as pdhg
 from conftest import golden, rel
 
 pytestmark = pytest.mark.gpu
