@@ -231,6 +231,31 @@ int taral_batch_info(const taral_batch* b, int* distinct_matrices, size_t* devic
 const char* taral_batch_last_error(const taral_batch* b);
 void taral_batch_destroy(taral_batch* b);
 
+/* ------------------------------------------------------------------------------------------------------------
+ * 6. KKT evaluation without device allocation. No counterpart in the reference: it is an addition for callers
+ *    that cannot call cudaMalloc -- a host whose GPU memory is reserved up front by another allocator, or a loop
+ *    that must not take cudaMalloc's implicit device synchronisation. It computes, on device vectors the caller
+ *    holds, the same 10 FP64 KKT scalars as pdhg_eval(ctx, 0, f, out) (same kernels, same fixed-order sums).
+ *
+ *    Scratch: a file-scope device array of 23,696 bytes (2 x 296 x 5 partial sums + 2 tickets), held by every GPU
+ *    that loads the library until the process exits. Every call shares it and it keeps the last call's contents;
+ *    each call clears the tickets that must start at zero. Calls whose work overlaps on the GPU (different streams,
+ *    threads or processes sharing the device) race on the array: serialise them. The first call on each device
+ *    looks up the array's device address (cudaGetSymbolAddress) with that device current; make that first call
+ *    before any stream capture. Nothing is allocated: no cudaMalloc, cudaFree or allocating library routine.
+ *
+ *    dtype: TARAL_FP64 (all 13 vectors double) or TARAL_FP32 (all float). Row vectors (length m): Ax, z, rl, ru,
+ *    Dr, zlast; column vectors (length n): x, ATz, c, l, u, Dc, xlast -- all device pointers, in the scaled space
+ *    of part 1. out10: device pointer to 10 doubles, written in the slot order of pdhg_eval. Asynchronous on
+ *    `stream` (NULL: the legacy default stream). m and n above TARAL_NOALLOC_MAX_DIM are rejected with
+ *    TARAL_ERR_INPUT (the kernels index with int and stride by 296 x 256).
+ * ------------------------------------------------------------------------------------------------------------ */
+#define TARAL_NOALLOC_MAX_DIM 2000000000
+int taral_kkt_eval_noalloc(int m, int n, int dtype, double f, const void* Ax, const void* z, const void* rl,
+                           const void* ru, const void* Dr, const void* zlast, const void* x, const void* ATz,
+                           const void* c, const void* l, const void* u, const void* Dc, const void* xlast,
+                           double* out10, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

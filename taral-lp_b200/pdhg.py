@@ -102,6 +102,8 @@ SIGNATURES = {
                                    C.POINTER(C.c_int64)]),
     "taral_batch_last_error": (C.c_char_p, [C.c_void_p]),
     "taral_batch_destroy": (None, [C.c_void_p]),
+    "taral_kkt_eval_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double] + [C.c_void_p] * 13 +
+                               [C.c_void_p, C.c_void_p]),
     "taral_spmv_plan_create": (C.c_int, [C.c_int, C.c_int, _lp, C.c_int, C.POINTER(C.c_void_p)]),
     "taral_spmv_run": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                  C.c_void_p]),
