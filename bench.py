@@ -179,13 +179,16 @@ def algorithmic_bytes(m, n, nnz, fp32=True):
 
 
 def traffic_from_profile():
-    p = ROOT / "profiles" / "roofline_traffic.json"
-    if p.exists():
-        try:
-            return json.loads(p.read_text())
-        except ValueError:
-            return None
-    return None
+    """DRAM bytes per launch of the row / column phase kernels from the committed ncu summary, or None."""
+    p = ROOT / "profiles" / "roofline_traffic.txt"
+    if not p.exists():
+        return None
+    out = {}
+    for line in p.read_text().splitlines():
+        parts = line.split()
+        if len(parts) == 2 and not line.startswith("#"):
+            out[parts[0]] = int(parts[1])
+    return out
 
 
 def our_arm(args, rank, world, dist):
@@ -257,9 +260,7 @@ def our_arm(args, rank, world, dist):
     peak, peak_kind = peaks()
     dom = "row" if row_ms >= col_ms else "col"
     tr = traffic_from_profile()
-    traffic = None
-    if tr and tr.get("kernel") == dom:
-        traffic = tr.get("dram_bytes_per_launch")
+    traffic = tr.get(dom) if tr else None
 
     if rank == 0:
         cpu = None

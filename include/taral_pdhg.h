@@ -174,9 +174,9 @@ int pdhg_create_model(const taral_model* md, int precision, int eval_freq, unsig
  * x0 / z0: optional start point (scaled space). out->device_s is the device time of the whole solve. */
 int pdhg_solve_ctx(pdhg_ctx* ctx, double bnorm, double cnorm, const taral_options* o, const double* x0,
                    const double* z0, taral_outcome* out, double* x, double* z);
-/* Measurement hook: `reps` iterations launched kernel by kernel, each row-phase (A x + dual step) and
- * column-phase (A^T z + primal step) kernel bracketed by CUDA events on the context stream. Returns the mean
- * milliseconds per launch of each. Advances the iteration state like pdhg_iterate(ctx, reps). */
+/* Measurement hook: `reps` launches of the row-phase kernel (A x + dual step) back to back, then `reps` of the
+ * column-phase kernel (A^T z + primal step), each run bracketed by CUDA events on the context stream. Returns the
+ * mean milliseconds per launch of each. Leaves the iterate in an unspecified state: start again before solving. */
 int pdhg_profile_phases(pdhg_ctx* ctx, int reps, double* row_ms, double* col_ms);
 
 /* ------------------------------------------------------------------------------------------------------------
@@ -230,6 +230,31 @@ int taral_batch_info(const taral_batch* b, int* distinct_matrices, size_t* devic
                      int64_t* nnz_total);
 const char* taral_batch_last_error(const taral_batch* b);
 void taral_batch_destroy(taral_batch* b);
+
+/* ------------------------------------------------------------------------------------------------------------
+ * 7. Learned warm start: an MLP (in -> hidden x depth with GELU -> out) trained and evaluated with this library's
+ *    own BF16 tensor-core kernels (FP32 accumulate), mapping a scenario's perturbation vector to an initial
+ *    (x, y) for taral_pdhg_solve_warm / taral_batch_solve. No counterpart in the reference.
+ *    Parameters, in order per layer: W (in x out, row-major) then b (out), FP32 on the host.
+ * ------------------------------------------------------------------------------------------------------------ */
+typedef struct taral_mlp taral_mlp;
+int taral_mlp_create(int in_dim, int hidden, int depth, int out_dim, int max_batch, taral_mlp** out);
+int64_t taral_mlp_param_count(const taral_mlp* h);
+int taral_mlp_set_params(taral_mlp* h, const float* params);
+int taral_mlp_get_params(taral_mlp* h, float* params);
+/* y (batch x out, host) = MLP(x (batch x in, host)). */
+int taral_mlp_forward(taral_mlp* h, int batch, const float* x, float* y);
+/* Loss mean((MLP(x) - target)^2) and its gradient with respect to every parameter (host, parameter order). */
+int taral_mlp_gradients(taral_mlp* h, int batch, const float* x, const float* target, double* loss, float* grads);
+/* Upload a training set once (count rows of x and target), then run Adam over shuffled mini-batches. */
+int taral_mlp_set_dataset(taral_mlp* h, int count, const float* x, const float* target);
+int taral_mlp_train(taral_mlp* h, int epochs, int batch, float lr, uint64_t seed, double* last_loss);
+const char* taral_mlp_last_error(const taral_mlp* h);
+void taral_mlp_destroy(taral_mlp* h);
+/* The MLP's GEMM on device buffers: C (M x N, f32) = op(A) op(B) with bf16 A, B; ta: A is stored K x M; tb: B is
+ * stored N x K; slices > 1: split-K with a workspace of slices * M * N floats. Asynchronous on `stream`. */
+int taral_gemm_bf16(int M, int N, int K, int ta, int tb, const void* A, const void* B, float* C, int slices,
+                    float* workspace, void* stream);
 
 /* ------------------------------------------------------------------------------------------------------------
  * 6. KKT evaluation without device allocation. No counterpart in the reference: it is an addition for callers

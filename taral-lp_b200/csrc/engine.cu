@@ -352,28 +352,21 @@ struct Engine final : EngineBase {
         return ms;
     }
     void profile_phases(int reps, double* row_ms, double* col_ms) override {
-        std::vector<cudaEvent_t> ev(size_t(4) * reps);
+        // reps row-phase launches back to back, then reps column-phase launches, each run bracketed by events:
+        // the mean includes the graph-free launch gap but not the event overhead of a single launch.
+        cudaEvent_t ev[3];
         for (auto& e : ev) CK(cudaEventCreate(&e));
-        k_xupd<T><<<grid_for(n), 256, 0, st>>>(n, x, ATz, c, l, u, par, xs);
-        ++launches;
-        for (int s = 0; s < reps; ++s) {
-            CK(cudaEventRecord(ev[4 * s], st));
-            rowblock(A, x, EpiRow<T>{Ax, z, zs, rl, ru, par});
-            CK(cudaEventRecord(ev[4 * s + 1], st));
-            CK(cudaEventRecord(ev[4 * s + 2], st));
-            rowblock(AT, z, EpiCol<T>{ATz, x, xs, c, l, u, par, s + 1 < reps ? 1 : 0});
-            CK(cudaEventRecord(ev[4 * s + 3], st));
-        }
+        CK(cudaEventRecord(ev[0], st));
+        for (int s = 0; s < reps; ++s) rowblock(A, x, EpiRow<T>{Ax, z, zs, rl, ru, par});
+        CK(cudaEventRecord(ev[1], st));
+        for (int s = 0; s < reps; ++s) rowblock(AT, z, EpiCol<T>{ATz, x, xs, c, l, u, par, 1});
+        CK(cudaEventRecord(ev[2], st));
         CK(cudaStreamSynchronize(st));
-        double r = 0, c2 = 0;
-        for (int s = 0; s < reps; ++s) {
-            float a, b;
-            CK(cudaEventElapsedTime(&a, ev[4 * s], ev[4 * s + 1]));
-            CK(cudaEventElapsedTime(&b, ev[4 * s + 2], ev[4 * s + 3]));
-            r += a, c2 += b;
-        }
+        float a, b;
+        CK(cudaEventElapsedTime(&a, ev[0], ev[1]));
+        CK(cudaEventElapsedTime(&b, ev[1], ev[2]));
         for (auto& e : ev) cudaEventDestroy(e);
-        *row_ms = r / reps, *col_ms = c2 / reps;
+        *row_ms = double(a) / reps, *col_ms = double(b) / reps;
     }
 };
 

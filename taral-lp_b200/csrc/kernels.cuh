@@ -21,6 +21,7 @@ constexpr int kThreads = 256;  // threads per CTA in every SpMV-shaped kernel
 constexpr int kTile = 2044;    // nonzeros staged per row block: with the 16-byte alignment slack, 512 quads
 constexpr int kRowsMax = 256;  // rows per row block (one epilogue row per thread)
 constexpr int kRedThreads = 256;
+constexpr int kMinBlocks = 8;   // resident CTAs per SM the SpMV kernels are compiled for (32 registers)
 
 template <class T>
 __device__ __forceinline__ T clampv(T v, T lo, T hi) { return v < lo ? lo : (v > hi ? hi : v); }
@@ -44,6 +45,18 @@ template <> struct Quad<double> {
 __device__ __forceinline__ void load_idx4(const int* p, int (&v)[4]) {
     asm volatile("ld.global.nc.L1::no_allocate.v4.s32 {%0,%1,%2,%3}, [%4];"
                  : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]) : "l"(p));
+}
+
+// Gathered vector entries are reused across rows and blocks: keep them in L1 as long as possible.
+__device__ __forceinline__ float gather(const float* p) {
+    float v;
+    asm volatile("ld.global.nc.L1::evict_last.f32 %0, [%1];" : "=f"(v) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ double gather(const double* p) {
+    double v;
+    asm volatile("ld.global.nc.L1::evict_last.f64 %0, [%1];" : "=d"(v) : "l"(p));
+    return v;
 }
 
 // Product type staged in shared memory: float products for a float matrix, double otherwise.
@@ -192,7 +205,7 @@ __device__ __forceinline__ void block_sums(const int* __restrict__ ptr, const in
 #pragma unroll
         for (int i = 0; i < kQuads; ++i)
 #pragma unroll
-            for (int e = 0; e < 4; ++e) g[i][e] = c[i][e] >= 0 ? __ldg(xin + c[i][e]) : X(0);
+            for (int e = 0; e < 4; ++e) g[i][e] = c[i][e] >= 0 ? gather(xin + c[i][e]) : X(0);
 #pragma unroll
         for (int i = 0; i < kQuads; ++i) {
             const int q = a0 + 4 * (tid + i * kThreads);
@@ -229,7 +242,7 @@ __device__ __forceinline__ void block_sums(const int* __restrict__ ptr, const in
 
 // One launch over all row blocks of one matrix; `skip` (may be NULL): return at once when *skip != 0.
 template <class T, class X, class E, bool VEC>
-__global__ void __launch_bounds__(kThreads) k_rowblock(const int* __restrict__ ptr, const int* __restrict__ idx,
+__global__ void __launch_bounds__(kThreads, kMinBlocks) k_rowblock(const int* __restrict__ ptr, const int* __restrict__ idx,
                                                          const T* __restrict__ val, const X* __restrict__ xin,
                                                          const int4* __restrict__ blk, const int* __restrict__ skip,
                                                          E epi) {
@@ -250,7 +263,7 @@ __global__ void __launch_bounds__(kThreads) k_rowblock(const int* __restrict__ p
 // offset, 0}: the block's rows r of the (possibly shared) matrix are rows r + shift of the concatenated instance
 // vectors, and its column indices address xin + offset. Blocks of instances with active[instance] == 0 return.
 template <class T, class X, class E, bool VEC>
-__global__ void __launch_bounds__(kThreads) k_rowblock_batch(const int* __restrict__ ptr, const int* __restrict__ idx,
+__global__ void __launch_bounds__(kThreads, kMinBlocks) k_rowblock_batch(const int* __restrict__ ptr, const int* __restrict__ idx,
                                                                const T* __restrict__ val, const X* __restrict__ xin,
                                                                const int4* __restrict__ blk,
                                                                const int4* __restrict__ ext,

@@ -104,6 +104,19 @@ SIGNATURES = {
     "taral_batch_destroy": (None, [C.c_void_p]),
     "taral_kkt_eval_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double] + [C.c_void_p] * 13 +
                                [C.c_void_p, C.c_void_p]),
+    "taral_mlp_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "taral_mlp_param_count": (C.c_int64, [C.c_void_p]),
+    "taral_mlp_set_params": (C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
+    "taral_mlp_get_params": (C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
+    "taral_mlp_forward": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    "taral_mlp_gradients": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float), _dp,
+                                      C.POINTER(C.c_float)]),
+    "taral_mlp_set_dataset": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    "taral_mlp_train": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_uint64, _dp]),
+    "taral_mlp_last_error": (C.c_char_p, [C.c_void_p]),
+    "taral_mlp_destroy": (None, [C.c_void_p]),
+    "taral_gemm_bf16": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                  C.c_int, C.c_void_p, C.c_void_p]),
     "taral_spmv_plan_create": (C.c_int, [C.c_int, C.c_int, _lp, C.c_int, C.POINTER(C.c_void_p)]),
     "taral_spmv_run": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                  C.c_void_p]),
@@ -365,6 +378,98 @@ class Batch:
     def close(self):
         if getattr(self, "h", None):
             lib().taral_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ------------------------------------------------------------------------------------------------ MLP
+_fp = C.POINTER(C.c_float)
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, np.float32)
+
+
+class Mlp:
+    """The learned warm start's network (taral_mlp_*): in -> hidden x depth (GELU) -> out, BF16 tensor-core GEMMs,
+    FP32 accumulate, Adam on FP32 master weights. Parameters are a flat float32 vector, per layer W (in x out) then
+    b."""
+
+    def __init__(self, in_dim, hidden, depth, out_dim, max_batch=256):
+        self.dims = (in_dim, hidden, depth, out_dim)
+        self.max_batch = max_batch
+        h = C.c_void_p()
+        _check(lib().taral_mlp_create(in_dim, hidden, depth, out_dim, max_batch, C.byref(h)))
+        self.h = h
+
+    def _err(self, code):
+        if code != OK:
+            raise TaralError(code, (lib().taral_mlp_last_error(self.h) or b"").decode())
+
+    @property
+    def param_count(self):
+        return lib().taral_mlp_param_count(self.h)
+
+    def shapes(self):
+        i, hd, d, o = self.dims
+        dims = [i] + [hd] * d + [o]
+        return [((dims[l], dims[l + 1]), (dims[l + 1],)) for l in range(d + 1)]
+
+    def init(self, seed=0):
+        """He-style initialisation: W ~ N(0, 2 / fan_in) (1 / fan_in for the output layer), b = 0."""
+        rng = np.random.default_rng(seed)
+        parts = []
+        sh = self.shapes()
+        for k, ((fi, fo), _) in enumerate(sh):
+            s = np.sqrt((1.0 if k == len(sh) - 1 else 2.0) / fi)
+            parts += [rng.standard_normal(fi * fo) * s, np.zeros(fo)]
+        self.set_params(np.concatenate(parts))
+
+    def set_params(self, p):
+        p = _f32(p)
+        assert p.size == self.param_count
+        self._err(lib().taral_mlp_set_params(self.h, p.ctypes.data_as(_fp)))
+
+    def get_params(self):
+        p = np.zeros(self.param_count, np.float32)
+        self._err(lib().taral_mlp_get_params(self.h, p.ctypes.data_as(_fp)))
+        return p
+
+    def forward(self, x):
+        x = _f32(np.atleast_2d(x))
+        y = np.zeros((x.shape[0], self.dims[3]), np.float32)
+        for b0 in range(0, x.shape[0], self.max_batch):
+            xb = _f32(x[b0:b0 + self.max_batch])
+            yb = np.zeros((xb.shape[0], self.dims[3]), np.float32)
+            self._err(lib().taral_mlp_forward(self.h, xb.shape[0], xb.ctypes.data_as(_fp), yb.ctypes.data_as(_fp)))
+            y[b0:b0 + xb.shape[0]] = yb
+        return y
+
+    def gradients(self, x, t):
+        x, t = _f32(x), _f32(t)
+        g = np.zeros(self.param_count, np.float32)
+        loss = C.c_double()
+        self._err(lib().taral_mlp_gradients(self.h, x.shape[0], x.ctypes.data_as(_fp), t.ctypes.data_as(_fp),
+                                            C.byref(loss), g.ctypes.data_as(_fp)))
+        return loss.value, g
+
+    def set_dataset(self, x, t):
+        x, t = _f32(x), _f32(t)
+        self._err(lib().taral_mlp_set_dataset(self.h, x.shape[0], x.ctypes.data_as(_fp), t.ctypes.data_as(_fp)))
+
+    def train(self, epochs, batch, lr, seed=0):
+        loss = C.c_double()
+        self._err(lib().taral_mlp_train(self.h, epochs, batch, lr, seed, C.byref(loss)))
+        return loss.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().taral_mlp_destroy(self.h)
             self.h = None
 
     def __del__(self):

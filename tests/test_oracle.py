@@ -105,3 +105,24 @@ def test_oracle_nan_cost_semantics(oracle_lib):
     lp.cost[0] = np.nan
     r, _, _ = oracle.solve(lp, tol=1e-6, max_iter=20000)
     assert r["status"] == "near_optimal" and np.isnan(r["objective"]) and np.isnan(r["rel_d"])
+
+
+def test_mlp_oracle_gradients_by_finite_differences():
+    """The numpy MLP restatement's analytic gradient agrees with central differences (no bf16 rounding)."""
+    import mlp_oracle
+    rng = np.random.default_rng(0)
+    shapes = [((5, 7), (7,)), ((7, 7), (7,)), ((7, 4), (4,))]
+    n = sum(a * b + b for (a, b), _ in shapes)
+    p = rng.standard_normal(n) * 0.4
+    x, t = rng.standard_normal((6, 5)), rng.standard_normal((6, 4))
+    saved = mlp_oracle.bf16
+    mlp_oracle.bf16 = lambda a: np.asarray(a, np.float64)
+    try:
+        _, g = mlp_oracle.loss_and_grads(p, shapes, x, t)
+        for i in rng.choice(n, 12, replace=False):
+            e = np.zeros(n)
+            e[i] = 1e-6
+            fd = (mlp_oracle.loss_and_grads(p + e, shapes, x, t)[0] - mlp_oracle.loss_and_grads(p - e, shapes, x, t)[0]) / 2e-6
+            assert abs(fd - g[i]) <= 1e-5 * max(1.0, abs(g[i]))
+    finally:
+        mlp_oracle.bf16 = saved
