@@ -20,6 +20,8 @@ the timed region, and the number of engine kernels launched in it.
   python bench.py [--gpus N] [--steps K] [--warmup W]        our engine
   python bench.py --impl reference ...                       the reference CPU PDHG (oracle/_ref/pdhg)
   python bench.py --profile-blocks B                         ncu capture mode: B blocks of 64 steps, no report
+  python bench.py --workload family [--instances 512]        the batched scenario family against the plain engine
+  python bench.py --workload warmstart [--train 512]         the learned warm start on the 24-period family
 """
 import argparse
 import json
@@ -296,6 +298,110 @@ def our_arm(args, rank, world, dist):
         print(json.dumps(line))
 
 
+def family_lps(count, seed=2024):
+    """The batched scenario family: `count` refinery LPs of 4 to 48 periods (seeded), prices and capacities scaled
+    by independent U(0.8, 1.2) factors. Returns (lps, periods)."""
+    import numpy as np
+    import lpgen
+    rng = np.random.default_rng(seed)
+    periods = rng.integers(4, 49, size=count)
+    base = lpgen.RefineryBase(48, seed=7)
+    P = lpgen.perturbations(count, seed=seed + 1)
+    return [base.instance(int(T), p) for T, p in zip(periods, P)], periods
+
+
+def family_arm(args):
+    """All scenarios in one batched context (FP32 iterates, FP64 per-instance restart state) against the plain
+    single-instance FP32 engine on a stratified sample of them; the plain per-LP time of the whole family is the
+    least-squares line in the number of periods through the sample, evaluated at every scenario's period count."""
+    import numpy as np
+    import pdhg
+    tol = WORKLOAD["tol"]
+    t0 = time.perf_counter()
+    lps, periods = family_lps(args.instances)
+    gen_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    b = pdhg.Batch(lps, tol=tol, precision=pdhg.FP32, time_limit=3000)
+    res, _, _ = b.solve(want_points=False)
+    batch_s = time.perf_counter() - t0
+    info = b.info()
+    b.close()
+    order = np.argsort(periods, kind="stable")
+    pick = order[np.linspace(0, len(order) - 1, min(args.sample, len(order))).round().astype(int)]
+    plain_t, plain_T, obj_diff = [], [], []
+    for i in pick:
+        t0 = time.perf_counter()
+        r, _, _ = pdhg.solve(lps[i], tol=tol, precision=pdhg.FP32, time_limit=600)
+        plain_t.append(time.perf_counter() - t0)
+        plain_T.append(int(periods[i]))
+        obj_diff.append(abs(r["objective"] - res[i]["objective"]) / max(1.0, abs(r["objective"])))
+        print(f"plain T={periods[i]} {plain_t[-1]:.3f}s it={r['iterations']} batched it={res[i]['iterations']}",
+              file=sys.stderr, flush=True)
+    slope, icpt = np.polyfit(np.array(plain_T, float), np.array(plain_t), 1)
+    plain_per_lp = float(np.mean(np.maximum(slope * periods + icpt, 0.0)))
+    k = len(lps)
+    its = [r["iterations"] for r in res]
+    line = {"metric": "time-to-1e-6 rel KKT per LP (batched scenario family)", "value": batch_s / k, "unit": "s",
+            "n_gpus": 1, "higher_is_better": False, "dtype": "fp32", "data": "synthetic",
+            "config": {"workload": f"refinery scenario family: {k} LPs of 4-48 periods (1,500 rows x 4,000 columns "
+                                   f"per period), prices and capacities x U(0.8,1.2), tol {tol}",
+                       "rows_total": int(sum(lp.m for lp in lps)), "cols_total": int(sum(lp.n for lp in lps)),
+                       "nnz_total": info["nnz_total"], "nnz_stored": info["nnz_stored"],
+                       "distinct_matrices": info["distinct_matrices"], "device_mem_bytes": info["device_mem_bytes"]},
+            "batched": {"wall_s": batch_s, "per_lp_s": batch_s / k, "device_s": res[0]["device_s"],
+                        "near_optimal": sum(r["status"] == "near_optimal" for r in res),
+                        "iterations_mean": float(np.mean(its)), "iterations_max": int(max(its))},
+            "plain_single_instance": {"per_lp_s_fit": plain_per_lp, "sample": len(pick),
+                                      "sample_periods": plain_T, "sample_s": plain_t,
+                                      "fit_s_per_period": float(slope), "fit_intercept_s": float(icpt)},
+            "speedup_per_lp": plain_per_lp / (batch_s / k),
+            "objective_max_rel_diff_batched_vs_plain": float(max(obj_diff)), "generate_s": gen_s}
+    print(json.dumps(line))
+
+
+def warmstart_arm(args):
+    """The learned warm start on the 24-period family: train on solutions of `--train` scenarios (seeds disjoint
+    from the evaluation seeds), then solve `--instances` held-out scenarios cold and warm (with the fallback
+    rule), all in batched contexts, and a sample of them with the plain single-instance engine."""
+    import numpy as np
+    import lpgen
+    import pdhg
+    import warmstart as W
+    T = 24
+    base = lpgen.RefineryBase(T, seed=7)
+    Ptr, Pev = lpgen.perturbations(args.train, seed=100), lpgen.perturbations(args.instances, seed=999)
+    t0 = time.perf_counter()
+    tr = [base.instance(T, p) for p in Ptr]
+    ev = [base.instance(T, p) for p in Pev]
+    gen_s = time.perf_counter() - t0
+    outs, xs, ys, data_s = W.solve_batch(tr, tol=1e-5)
+    t0 = time.perf_counter()
+    ws = W.train(Ptr, xs, ys, np.array([r["primal_weight"] for r in outs]), epochs=args.epochs, batch=256, lr=1e-3)
+    train_s = time.perf_counter() - t0
+    del xs, ys
+    res = W.evaluate(ev, Pev, ws, tol=WORKLOAD["tol"])
+    plain = []
+    for i in range(min(args.sample, len(ev))):
+        r, _, _ = pdhg.solve(ev[i], tol=WORKLOAD["tol"], precision=pdhg.FP32, time_limit=600)
+        plain.append(r["solve_s"])
+    k = len(ev)
+    warm_total = res["warm_s"] + res["probe_s"] + res["predict_s"]
+    line = {"metric": "time-to-1e-6 rel KKT per LP (learned warm start, batched)", "value": warm_total / k,
+            "unit": "s", "n_gpus": 1, "higher_is_better": False, "dtype": "fp32", "data": "synthetic",
+            "config": {"workload": f"refinery family, {T} periods ({ev[0].m} rows x {ev[0].n} columns), "
+                                   f"{args.train} training / {k} held-out scenarios (disjoint seeds)",
+                       "mlp": f"256 -> 512 x 3 (GELU) -> {ev[0].n + ev[0].m + 1}, bf16 weights, fp32 accumulate"},
+            "train": {"solutions_s": data_s, "train_s": train_s, "final_loss": ws.net.last_loss,
+                      "generate_s": gen_s, "epochs": args.epochs},
+            "cold": {"per_lp_s": res["cold_s"] / k, "iterations_mean": float(np.mean(res["cold_iterations"]))},
+            "warm": {"per_lp_s": warm_total / k, "iterations_mean": float(np.mean(res["warm_iterations"])),
+                     "used_warm": int(sum(res["used_warm"])), "probe_s": res["probe_s"]},
+            "plain_single_instance_per_lp_s": float(np.mean(plain)) if plain else None,
+            "objective_max_rel_diff_warm_vs_cold": float(max(abs(a - b) / max(1.0, abs(a)) for a, b in
+                                                             zip(res["cold_objective"], res["warm_objective"])))}
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -304,12 +410,23 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--profile-blocks", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", choices=["lp", "family", "warmstart"], default="lp",
+                    help="lp: the single large LP (the bench line); family: the batched scenario family; "
+                         "warmstart: the learned warm start on the 24-period family")
+    ap.add_argument("--instances", type=int, default=512)
+    ap.add_argument("--sample", type=int, default=12)
+    ap.add_argument("--train", type=int, default=512)
+    ap.add_argument("--epochs", type=int, default=200)
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     dist = world > 1
     if args.impl == "reference":
         reference_arm(args, rank, world)
+        return
+    if args.workload in ("family", "warmstart"):
+        if rank == 0:
+            (family_arm if args.workload == "family" else warmstart_arm)(args)
         return
     if dist:
         import datetime

@@ -221,10 +221,11 @@ typedef struct taral_batch taral_batch;
  * point into must stay valid until taral_batch_destroy (the final original-space check reads them). */
 int taral_batch_create(const taral_model* models, int count, const taral_options* o, taral_batch** out);
 /* Solve all instances. x0[i] / y0[i]: optional warm start of instance i (original space, y in the minimisation
- * form), x0 / y0 themselves may be NULL. outs[i]: instance i's outcome (solve_s and device_s are the whole
- * batch's). x_out[i] (n_i) / y_out[i] (m_i) may be NULL, as may x_out / y_out. */
-int taral_batch_solve(taral_batch* b, const double* const* x0, const double* const* y0, taral_outcome* outs,
-                      double* const* x_out, double* const* y_out);
+ * form), x0 / y0 themselves may be NULL. w0: NULL, or per instance the initial primal weight (a value that is not
+ * finite and positive keeps the default ||c|| / ||b|| of gpu/pdhg.cu:776). outs[i]: instance i's outcome (solve_s
+ * and device_s are the whole batch's). x_out[i] (n_i) / y_out[i] (m_i) may be NULL, as may x_out / y_out. */
+int taral_batch_solve(taral_batch* b, const double* const* x0, const double* const* y0, const double* w0,
+                      taral_outcome* outs, double* const* x_out, double* const* y_out);
 /* Distinct stored matrices, device bytes, nonzeros stored and nonzeros over all instances. */
 int taral_batch_info(const taral_batch* b, int* distinct_matrices, size_t* device_mem, int64_t* nnz_stored,
                      int64_t* nnz_total);
@@ -255,6 +256,10 @@ void taral_mlp_destroy(taral_mlp* h);
  * stored N x K; slices > 1: split-K with a workspace of slices * M * N floats. Asynchronous on `stream`. */
 int taral_gemm_bf16(int M, int N, int K, int ta, int tb, const void* A, const void* B, float* C, int slices,
                     float* workspace, void* stream);
+/* The MLP's forward GEMM on the tcgen05 tensor cores (accumulator in tensor memory): C (M x N, f32) = A Bt^T with
+ * A (M x K) and Bt (N x K) bf16, row-major, 16-byte aligned, K a multiple of 8. err: a device int that is set to 1
+ * if a completion wait gave up (C is then undefined); it is never cleared here. Asynchronous on `stream`. */
+int taral_gemm_bf16_tc(int M, int N, int K, const void* A, const void* Bt, float* C, int* err, void* stream);
 
 /* ------------------------------------------------------------------------------------------------------------
  * 6. KKT evaluation without device allocation. No counterpart in the reference: it is an addition for callers

@@ -328,7 +328,8 @@ uint64_t fnv(const void* p, size_t n, uint64_t h) {
 
 struct BatchBase {
     virtual ~BatchBase() = default;
-    virtual void solve(const double* const* x0, const double* const* y0, taral_outcome* outs, double* const* xo,
+    virtual void solve(const double* const* x0, const double* const* y0, const double* w0, taral_outcome* outs,
+                       double* const* xo,
                        double* const* yo) = 0;
     std::string err;
     int distinct = 0;
@@ -583,8 +584,8 @@ struct Batch final : BatchBase {
         launches += 7;
     }
 
-    void solve(const double* const* x0, const double* const* y0, taral_outcome* outs, double* const* xo,
-               double* const* yo) override {
+    void solve(const double* const* x0, const double* const* y0, const double* w0, taral_outcome* outs,
+               double* const* xo, double* const* yo) override {
         auto t0 = Clock::now();
         cudaEvent_t e0, e1;
         BK(cudaEventCreate(&e0));
@@ -647,6 +648,7 @@ struct Batch final : BatchBase {
             q.norm = norms[i];
             q.eta = norms[i] > 0 ? 0.95 / norms[i] : 1.0;
             q.w = cs > 1e-10 && bs > 1e-10 ? cs / bs : 1.0;
+            if (w0 && std::isfinite(w0[i]) && w0[i] > 0) q.w = w0[i];  // caller's initial primal weight
             q.bnorm = v.bnorm, q.cnorm = v.cnorm, q.running = 1, q.status = TARAL_ITERATION_LIMIT;
             q.best_p = q.best_d = q.best_g = kInf;
             hpar[2 * i] = q.eta / q.w, hpar[2 * i + 1] = q.eta * q.w;
@@ -797,10 +799,10 @@ extern "C" int taral_batch_create(const taral_model* models, int count, const ta
 }
 
 extern "C" int taral_batch_solve(taral_batch* h, const double* const* x0, const double* const* y0,
-                                 taral_outcome* outs, double* const* x_out, double* const* y_out) {
+                                 const double* w0, taral_outcome* outs, double* const* x_out, double* const* y_out) {
     if (!h || !outs) return TARAL_ERR_INPUT;
     try {
-        h->b->solve(x0, y0, outs, x_out, y_out);
+        h->b->solve(x0, y0, w0, outs, x_out, y_out);
     } catch (const taral::BatchError& e) {
         h->b->err = e.msg;
         return TARAL_ERR_CUDA;

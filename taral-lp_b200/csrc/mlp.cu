@@ -6,9 +6,12 @@
 // Forward per layer: C = H_{l-1} W_l (GEMM, FP32 accumulate), Z = C + b, H = bf16(gelu(Z)) (last layer: Y = Z).
 // Backward: dW = H_{l-1}^T dZ, db = sum_b dZ, dH_{l-1} = dZ W_l^T, dZ = dH * gelu'(Z); loss = mean (Y - T)^2.
 //
-// GEMM: mma.sync m16n8k16 (bf16 x bf16 -> f32), 128 x 128 x 32 CTA tiles, 8 warps of 64 x 32, operands staged in
-// shared memory and fed with ldmatrix; A may be stored transposed (TA: A = X^T) and B as [N][K] (TB: B = W^T);
-// split-K writes per-slice partials that a second kernel adds in slice order (deterministic).
+// GEMMs: the forward pass runs on the tcgen05 tensor cores (mlp_tc.cu: C = H Wt^T with Wt = W^T kept as a bf16
+// [out][in] copy, refreshed whenever the weights change) for every layer whose input width is a multiple of 8.
+// The backward pass (and any other layer) uses mma.sync m16n8k16 (bf16 x bf16 -> f32), 128 x 128 x 32 CTA tiles,
+// 8 warps of 64 x 32, operands staged in shared memory and fed with ldmatrix; A may be stored transposed (TA: A =
+// X^T) and B as [N][K] (TB: B = W^T); split-K writes per-slice partials that a second kernel adds in slice order
+// (deterministic).
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -23,6 +26,9 @@
 #include "../../include/taral_pdhg.h"
 
 namespace taral {
+namespace tc {
+int gemm_tc(int M, int N, int K, const void* A, const void* Bt, float* C, int* err, cudaStream_t stream);
+}
 namespace mlp {
 
 using bf16 = __nv_bfloat16;
@@ -243,6 +249,21 @@ __global__ void k_adam(size_t n, float* __restrict__ w, const float* __restrict_
     }
 }
 
+// Wt[c][r] = W[r][c] for W rows x cols (bf16), through a 32 x 32 shared-memory tile.
+__global__ void k_transpose(int rows, int cols, const bf16* __restrict__ W, bf16* __restrict__ Wt) {
+    __shared__ bf16 t[32][33];
+    const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32, tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    for (int i = ty; i < 32; i += 8) {
+        const int r = r0 + i, c = c0 + tx;
+        if (r < rows && c < cols) t[i][tx] = W[size_t(r) * cols + c];
+    }
+    __syncthreads();
+    for (int i = ty; i < 32; i += 8) {
+        const int c = c0 + i, r = r0 + tx;
+        if (r < rows && c < cols) Wt[size_t(c) * rows + r] = t[tx][i];
+    }
+}
+
 // Gather dataset rows idx[0..rows) into contiguous batch buffers.
 __global__ void k_gather_rows(int rows, int cols, const int* __restrict__ idx, const float* __restrict__ src,
                               float* __restrict__ dst, bf16* __restrict__ dstb) {
@@ -262,6 +283,7 @@ struct Layer {
     float *W = nullptr, *b = nullptr, *gW = nullptr, *gb = nullptr, *mW = nullptr, *vW = nullptr, *mb = nullptr,
           *vb = nullptr;
     bf16* Wb = nullptr;
+    bf16* Wt = nullptr;  // W^T [out][in] (the tcgen05 forward GEMM's K-major B operand); null: forward on mma.sync
     float* Z = nullptr;  // pre-activation [batch][out]
     bf16* H = nullptr;   // activation [batch][out] (GEMM operand of the next layer)
 };
@@ -274,6 +296,7 @@ struct Mlp {
     bf16 *dYb = nullptr, *dZb = nullptr;
     double* part = nullptr;
     int* d_idx = nullptr;
+    int* d_err = nullptr;  // set by the tcgen05 GEMM when a completion wait gave up
     float *DX = nullptr, *DT = nullptr;  // dataset
     int dcount = 0;
     size_t ws_count = 0;
@@ -306,6 +329,7 @@ struct Mlp {
             size_t nw = size_t(y.in) * y.out;
             y.W = alloc<float>(nw), y.gW = alloc<float>(nw), y.mW = alloc<float>(nw), y.vW = alloc<float>(nw);
             y.Wb = alloc<bf16>(nw);
+            if (y.in % 8 == 0) y.Wt = alloc<bf16>(nw);
             y.b = alloc<float>(y.out), y.gb = alloc<float>(y.out), y.mb = alloc<float>(y.out), y.vb = alloc<float>(y.out);
             y.Z = alloc<float>(size_t(mb) * y.out), y.H = alloc<bf16>(size_t(mb) * y.out);
             MK(cudaMemsetAsync(y.mW, 0, nw * sizeof(float), s));
@@ -319,7 +343,8 @@ struct Mlp {
         Xb = alloc<bf16>(size_t(mb) * in), Xf = alloc<float>(size_t(mb) * in), Tf = alloc<float>(size_t(mb) * out);
         C = alloc<float>(size_t(mb) * widest), R = alloc<float>(size_t(mb) * out), dYb = alloc<bf16>(size_t(mb) * out);
         dHf = alloc<float>(size_t(mb) * widest), dZf = alloc<float>(size_t(mb) * hid), dZb = alloc<bf16>(size_t(mb) * hid);
-        part = alloc<double>(mb), d_idx = alloc<int>(mb);
+        part = alloc<double>(mb), d_idx = alloc<int>(mb), d_err = alloc<int>(1);
+        MK(cudaMemsetAsync(d_err, 0, sizeof(int), s));
         ws_count = size_t(64) * mb * hid;  // split-K partials of dH = dZ W^T (K = out)
         ws = alloc<float>(ws_count);
         MK(cudaStreamSynchronize(s));
@@ -348,11 +373,35 @@ struct Mlp {
         MK(cudaGetLastError());
     }
 
+    void refresh_transposes() {  // Wt = Wb^T for the layers whose forward GEMM runs on tcgen05
+        for (Layer& y : L)
+            if (y.Wt) {
+                dim3 grid((y.out + 31) / 32, (y.in + 31) / 32);
+                k_transpose<<<grid, 256, 0, s>>>(y.in, y.out, y.Wb, y.Wt);
+            }
+        MK(cudaGetLastError());
+    }
+
+    void check_tc() {  // after a stream synchronisation: did a tcgen05 GEMM give up waiting?
+        int e = 0;
+        MK(cudaMemcpyAsync(&e, d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
+        MK(cudaStreamSynchronize(s));
+        if (e) {
+            MK(cudaMemsetAsync(d_err, 0, sizeof(int), s));
+            throw MlpError{"tcgen05 GEMM: an MMA completion wait timed out"};
+        }
+    }
+
     void forward(int batch) {  // Xb -> L[l].Z, L[l].H ; output Z of the last layer is Y
         const bf16* in = Xb;
         for (int l = 0; l <= depth; ++l) {
             Layer& y = L[l];
-            gemm<false, false>(batch, y.out, y.in, in, y.Wb, C);
+            if (y.Wt) {
+                if (taral::tc::gemm_tc(batch, y.out, y.in, in, y.Wt, C, d_err, s) != TARAL_OK)
+                    throw MlpError{std::string("tcgen05 GEMM launch: ") + cudaGetErrorString(cudaGetLastError())};
+            } else {
+                gemm<false, false>(batch, y.out, y.in, in, y.Wb, C);
+            }
             k_bias_act<<<grid1(size_t(batch) * y.out), 256, 0, s>>>(batch, y.out, C, y.b, y.Z, l < depth ? y.H : nullptr,
                                                                     l < depth ? 1 : 0);
             in = y.H;
@@ -395,7 +444,7 @@ struct Mlp {
             k_adam<<<grid1(nw), 256, 0, s>>>(nw, y.W, y.gW, y.mW, y.vW, y.Wb, lr, b1, b2, eps, c1, c2);
             k_adam<<<grid1(y.out), 256, 0, s>>>(y.out, y.b, y.gb, y.mb, y.vb, nullptr, lr, b1, b2, eps, c1, c2);
         }
-        MK(cudaGetLastError());
+        refresh_transposes();
     }
 
     void load_input(int batch, const float* x_host) {
@@ -458,6 +507,7 @@ extern "C" int taral_mlp_set_params(taral_mlp* h, const float* params) {
             MK(cudaMemcpyAsync(y.b, p, y.out * sizeof(float), cudaMemcpyHostToDevice, m.s));
             p += y.out;
         }
+        m.refresh_transposes();
         MK(cudaStreamSynchronize(m.s));
     })
 }
@@ -486,6 +536,7 @@ extern "C" int taral_mlp_forward(taral_mlp* h, int batch, const float* x, float*
         m.forward(batch);
         MK(cudaMemcpyAsync(y, m.L[m.depth].Z, size_t(batch) * m.out_dim * sizeof(float), cudaMemcpyDeviceToHost, m.s));
         MK(cudaStreamSynchronize(m.s));
+        m.check_tc();
     })
 }
 
@@ -498,6 +549,7 @@ extern "C" int taral_mlp_gradients(taral_mlp* h, int batch, const float* x, cons
         MK(cudaMemcpyAsync(m.Tf, target, size_t(batch) * m.out_dim * sizeof(float), cudaMemcpyHostToDevice, m.s));
         m.forward(batch);
         double l = m.backward(batch);
+        m.check_tc();
         if (loss) *loss = l;
         if (grads) {
             float* p = grads;
@@ -549,6 +601,7 @@ extern "C" int taral_mlp_train(taral_mlp* h, int epochs, int batch, float lr, ui
                 m.adam(lr);
             }
         }
+        m.check_tc();
         if (last_loss) *last_loss = loss;
     })
 }

@@ -97,7 +97,8 @@ SIGNATURES = {
     "taral_mps_name": (C.c_char_p, [C.c_void_p]),
     "taral_mps_free": (None, [C.c_void_p]),
     "taral_batch_create": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(OptionsT), C.POINTER(C.c_void_p)]),
-    "taral_batch_solve": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "taral_batch_solve": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                    C.c_void_p]),
     "taral_batch_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_size_t), C.POINTER(C.c_int64),
                                    C.POINTER(C.c_int64)]),
     "taral_batch_last_error": (C.c_char_p, [C.c_void_p]),
@@ -117,6 +118,8 @@ SIGNATURES = {
     "taral_mlp_destroy": (None, [C.c_void_p]),
     "taral_gemm_bf16": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
                                   C.c_int, C.c_void_p, C.c_void_p]),
+    "taral_gemm_bf16_tc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                     C.c_void_p]),
     "taral_spmv_plan_create": (C.c_int, [C.c_int, C.c_int, _lp, C.c_int, C.POINTER(C.c_void_p)]),
     "taral_spmv_run": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                  C.c_void_p]),
@@ -346,9 +349,9 @@ class Batch:
         return {"distinct_matrices": d.value, "device_mem_bytes": mem.value, "nnz_stored": ns.value,
                 "nnz_total": nt.value}
 
-    def solve(self, x0=None, y0=None, want_points=True):
+    def solve(self, x0=None, y0=None, want_points=True, w0=None):
         """Returns (list of outcome dicts, list of x, list of y). x0 / y0: optional lists of warm starts (entries
-        may be None)."""
+        may be None); w0: optional initial primal weights (entries <= 0 keep the default)."""
         k = len(self.lps)
         outs = (OutcomeT * k)()
 
@@ -362,8 +365,11 @@ class Batch:
         xout = [np.zeros(max(lp.n, 1)) for lp in self.lps] if want_points else None
         yout = [np.zeros(max(lp.m, 1)) for lp in self.lps] if want_points else None
         tabs = [table(v) for v in (xin, yin, xout, yout)]
-        code = lib().taral_batch_solve(self.h, tabs[0][1], tabs[1][1], C.cast(outs, C.c_void_p), tabs[2][1],
-                                       tabs[3][1])
+        wv = None if w0 is None else _f64(np.nan_to_num(np.asarray(w0, np.float64), nan=0.0))
+        if wv is not None and wv.size != k:
+            raise ValueError("w0 needs one entry per instance")
+        code = lib().taral_batch_solve(self.h, tabs[0][1], tabs[1][1], None if wv is None else wv.ctypes.data,
+                                       C.cast(outs, C.c_void_p), tabs[2][1], tabs[3][1])
         if code != OK:
             raise TaralError(code, (lib().taral_batch_last_error(self.h) or b"").decode())
         res = []
@@ -420,13 +426,14 @@ class Mlp:
         dims = [i] + [hd] * d + [o]
         return [((dims[l], dims[l + 1]), (dims[l + 1],)) for l in range(d + 1)]
 
-    def init(self, seed=0):
-        """He-style initialisation: W ~ N(0, 2 / fan_in) (1 / fan_in for the output layer), b = 0."""
+    def init(self, seed=0, out_scale=1.0):
+        """He-style initialisation: W ~ N(0, 2 / fan_in) (out_scale^2 / fan_in for the output layer), b = 0.
+        out_scale = 0 starts the network at a zero output (with normalised targets: the training mean)."""
         rng = np.random.default_rng(seed)
         parts = []
         sh = self.shapes()
         for k, ((fi, fo), _) in enumerate(sh):
-            s = np.sqrt((1.0 if k == len(sh) - 1 else 2.0) / fi)
+            s = np.sqrt((out_scale ** 2 if k == len(sh) - 1 else 2.0) / fi)
             parts += [rng.standard_normal(fi * fo) * s, np.zeros(fo)]
         self.set_params(np.concatenate(parts))
 

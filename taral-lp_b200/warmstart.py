@@ -2,9 +2,10 @@
 
 A scenario is the family's base LP with its prices and capacities scaled by a 256-vector p of factors in
 [0.8, 1.2] (lpgen.RefineryBase.instance). The network maps the normalised p to the normalised optimal (x, y) of
-that scenario; it is trained on solutions the batched PDHG engine itself computes, with this library's own BF16
-tensor-core kernels (pdhg.Mlp). At solve time the prediction is projected onto the column bounds and handed to
-the solver as its start point.
+that scenario and to the logarithm of the primal weight that scenario's solve ended with; it is trained on
+solutions the batched PDHG engine itself computes, with this library's own BF16 tensor-core kernels (pdhg.Mlp). At
+solve time x is projected onto the column bounds, and (x, y, w) are handed to the solver as its start point and
+initial primal weight.
 
 Fallback: the unmodified cold start stays the default. For each scenario the warm and the cold start are both run
 for one evaluation block (64 iterations); if the warm start's relative KKT error after that block is not better
@@ -53,7 +54,7 @@ def kkt(r: dict) -> float:
 
 
 def solve_batch(lps, tol, precision=pdhg.FP32, x0=None, y0=None, max_iter=2_000_000_000, time_limit=3600.0,
-                chunk=256):
+                chunk=256, w0=None):
     """Solve many scenarios in batches of `chunk` (one context per chunk). Returns (outcomes, xs, ys, seconds)."""
     outs, xs, ys = [], [], []
     t = 0.0
@@ -62,8 +63,9 @@ def solve_batch(lps, tol, precision=pdhg.FP32, x0=None, y0=None, max_iter=2_000_
         b = pdhg.Batch(part, tol=tol, precision=precision, max_iter=max_iter, time_limit=time_limit)
         px = None if x0 is None else x0[c0:c0 + chunk]
         py = None if y0 is None else y0[c0:c0 + chunk]
+        pw = None if w0 is None else w0[c0:c0 + chunk]
         t0 = time.perf_counter()
-        r, x, y = b.solve(x0=px, y0=py)
+        r, x, y = b.solve(x0=px, y0=py, w0=pw)
         t += time.perf_counter() - t0
         outs += r
         xs += x
@@ -80,18 +82,21 @@ class WarmStart:
     m: int
 
     def predict(self, P: np.ndarray, lps: List[lpgen.LP]):
+        """Predicted (x, y, w) per scenario: x projected onto the column bounds, w the initial primal weight."""
         Z = self.net.forward(features(P))
         T = self.norm.decode(Z.astype(np.float64))
-        xs, ys = [], []
+        xs, ys, ws = [], [], []
         for t, lp in zip(T, lps):
             xs.append(np.clip(t[:self.n], lp.col_lo, lp.col_up))
             ys.append(t[self.n:self.n + self.m])
-        return xs, ys
+            ws.append(float(np.exp(np.clip(t[self.n + self.m], -30.0, 30.0))))
+        return xs, ys, np.array(ws)
 
 
-def train(P: np.ndarray, X: List[np.ndarray], Y: List[np.ndarray], hidden=512, depth=3, epochs=200, batch=256,
-          lr=1e-3, seed=0) -> WarmStart:
-    T = np.hstack([np.vstack(X), np.vstack(Y)])
+def train(P: np.ndarray, X: List[np.ndarray], Y: List[np.ndarray], W: np.ndarray, hidden=512, depth=3, epochs=200,
+          batch=256, lr=1e-3, seed=0) -> WarmStart:
+    """Fit the network to (x, y, log w) of solved scenarios (W: their final primal weights)."""
+    T = np.hstack([np.vstack(X), np.vstack(Y), np.log(np.asarray(W, np.float64))[:, None]])
     norm = Normalizer.fit(T)
     batch = min(batch, len(P))
     net = pdhg.Mlp(P.shape[1], hidden, depth, T.shape[1], max_batch=batch)
@@ -109,15 +114,16 @@ def evaluate(lps, P, ws: Optional[WarmStart], tol=1e-6, precision=pdhg.FP32, pro
     if ws is None:
         return res
     t0 = time.perf_counter()
-    x0, y0 = ws.predict(P, lps)
+    x0, y0, w0 = ws.predict(P, lps)
     t_pred = time.perf_counter() - t0
     # fallback probe: one block from each start
-    pw, _, _, t_pw = solve_batch(lps, tol, precision, x0=x0, y0=y0, max_iter=probe_iters)
+    pw, _, _, t_pw = solve_batch(lps, tol, precision, x0=x0, y0=y0, w0=w0, max_iter=probe_iters)
     pc, _, _, t_pc = solve_batch(lps, tol, precision, max_iter=probe_iters)
     use = [kkt(a) < kkt(b) for a, b in zip(pw, pc)]
     wx = [x if u else None for x, u in zip(x0, use)]
     wy = [y if u else None for y, u in zip(y0, use)]
-    warm, _, _, t_warm = solve_batch(lps, tol, precision, x0=wx, y0=wy)
+    ww = np.where(use, w0, 0.0)
+    warm, _, _, t_warm = solve_batch(lps, tol, precision, x0=wx, y0=wy, w0=ww)
     res.update({"warm_iterations": [r["iterations"] for r in warm], "warm_status": [r["status"] for r in warm],
                 "warm_s": t_warm, "predict_s": t_pred, "probe_s": t_pw + t_pc, "used_warm": use,
                 "warm_objective": [r["objective"] for r in warm]})

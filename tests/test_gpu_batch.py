@@ -58,6 +58,13 @@ def test_batch_warm_start_and_limits(engine_lib):
     res3, _, _ = b.solve(x0=[xs[0], None, None], y0=[ys[0], None, None])  # only instance 0 warm
     assert res3[0]["iterations"] < res[0]["iterations"] / 4
     assert [r["iterations"] for r in res3[1:]] == [r["iterations"] for r in res[1:]]
+    # initial primal weight: values that are not finite and positive keep the default
+    res5, _, _ = b.solve(w0=[0.0, float("nan"), -1.0])
+    assert [r["iterations"] for r in res5] == [r["iterations"] for r in res]
+    res6, _, _ = b.solve(w0=[r["primal_weight"] * 8.0 for r in res])
+    for r, r6 in zip(res, res6):
+        assert r6["status"] == "near_optimal" and rel(r6["objective"], r["objective"]) < 1e-5
+    assert [r["iterations"] for r in res6] != [r["iterations"] for r in res]
     b2 = pdhg.Batch(lps, tol=1e-12, max_iter=128, time_limit=120)
     res4, _, _ = b2.solve()
     assert all(r["status"] == "iteration_limit" and r["iterations"] == 128 for r in res4)
