@@ -24,6 +24,7 @@
 #include "engine.hpp"
 #include "host.hpp"
 #include "kernels.cuh"
+#include "scaling.cuh"
 
 namespace taral {
 
@@ -133,11 +134,10 @@ struct Engine final : EngineBase {
         return d;
     }
 
-    void init(const taral_csr& hA, const taral_csr& hAT, const double* hc_ptr, const double* hl, const double* hu,
-              const double* hrl_ptr, const double* hru_ptr, const double* hDr, const double* hDc, int m_, int n_,
-              int freq, unsigned flags) {
+    size_t free0 = 0;
+    void begin(int m_, int n_, int freq, unsigned flags) {
         m = m_, n = n_, eval_freq = std::max(1, freq), use_graph = !(flags & TARAL_FLAG_NO_GRAPH);
-        size_t free0, free1, total;
+        size_t total;
         CK(cudaMemGetInfo(&free0, &total));
         int dev;
         CK(cudaGetDevice(&dev));
@@ -145,7 +145,91 @@ struct Engine final : EngineBase {
         CK(cudaGetDeviceProperties(&prop, dev));
         name = prop.name;
         CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    }
+    void init(const taral_csr& hA, const taral_csr& hAT, const double* hc_ptr, const double* hl, const double* hu,
+              const double* hrl_ptr, const double* hru_ptr, const double* hDr, const double* hDc, int m_, int n_,
+              int freq, unsigned flags) {
+        begin(m_, n_, freq, flags);
         A = upload(hA), AT = upload(hAT);
+        nnz = hA.nnz;
+        finish_init(hc_ptr, hl, hu, hrl_ptr, hru_ptr, hDr, hDc);
+    }
+    // Row pointers, column indices and row blocks of one matrix on the device; the values are left to the caller.
+    DevMat upload_structure(const Csr& a) {
+        DevMat d;
+        d.rows = a.rows, d.nnz = int64_t(a.idx.size());
+        std::vector<int> p32(size_t(a.rows) + 1);
+        for (int r = 0; r <= a.rows; ++r) p32[r] = int(a.ptr[r]);
+        std::vector<int4> blk = build_row_blocks(a.ptr.data(), a.rows);
+        d.nblk = int(blk.size());
+        d.ptr = alloc<int>(p32.size()), d.idx = alloc<int>(size_t(d.nnz)), d.blk = alloc<int4>(blk.size());
+        CK(cudaMemcpyAsync(d.ptr, p32.data(), p32.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+        if (d.nnz) CK(cudaMemcpyAsync(d.idx, a.idx.data(), size_t(d.nnz) * sizeof(int), cudaMemcpyHostToDevice, st));
+        if (!blk.empty())
+            CK(cudaMemcpyAsync(d.blk, blk.data(), blk.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
+        d.val = alloc<T>(size_t(d.nnz));
+        CK(cudaStreamSynchronize(st));  // the host vectors may be released after return
+        return d;
+    }
+    // Set-up from the column-wise model with the scaling on the device (scaling.cuh): the host builds the unscaled
+    // A and A^T (model_matrices, the reference's transposes), the device scales them in FP64 and narrows the values
+    // to T in place. Fills P's Dr, Dc, vectors and norms (scale_vectors on the host, O(m + n)) and nnz; P.A and
+    // P.AT stay empty. host_s: seconds of host work.
+    void init_model(const taral_model& md, double sign, Scaled& P, int freq, unsigned flags, double* host_s) {
+        auto t0 = Clock::now();
+        Csr hA, hAT;
+        model_matrices(md, hA, hAT);
+        double hs = since(t0);
+        begin(md.m, md.n, freq, flags);
+        A = upload_structure(hA), AT = upload_structure(hAT);
+        const int64_t nz = int64_t(hA.val.size());
+        P.m = m, P.n = n;
+        P.Dr.resize(size_t(m)), P.Dc.resize(size_t(n));
+        {
+        double *va = nullptr, *vt = nullptr, *dr = nullptr, *dc = nullptr, *rs = nullptr, *cs = nullptr;
+        struct Scratch {  // FP64 working values and factors, released when the set-up ends
+            std::vector<void*> p;
+            ~Scratch() { for (void* q : p) cudaFree(q); }
+        } tmp;
+        auto scratch = [&](size_t count) {
+            void* q = nullptr;
+            CK(cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(double)));
+            tmp.p.push_back(q);
+            return static_cast<double*>(q);
+        };
+        if (sizeof(T) == sizeof(double)) {
+            va = reinterpret_cast<double*>(A.val), vt = reinterpret_cast<double*>(AT.val);
+        } else {
+            va = scratch(size_t(nz)), vt = scratch(size_t(nz));
+        }
+        dr = scratch(size_t(m)), dc = scratch(size_t(n)), rs = scratch(size_t(m)), cs = scratch(size_t(n));
+        if (nz) {
+            CK(cudaMemcpyAsync(va, hA.val.data(), size_t(nz) * sizeof(double), cudaMemcpyHostToDevice, st));
+            CK(cudaMemcpyAsync(vt, hAT.val.data(), size_t(nz) * sizeof(double), cudaMemcpyHostToDevice, st));
+        }
+        scale_on_device(m, n, A.ptr, A.idx, va, AT.ptr, AT.idx, vt, dr, dc, rs, cs, st);
+        if (sizeof(T) != sizeof(double) && nz) {
+            const int g = int(std::min<int64_t>((nz + 255) / 256, 148 * 16));
+            k_narrow<T><<<g, 256, 0, st>>>(nz, va, static_cast<T*>(A.val));
+            k_narrow<T><<<g, 256, 0, st>>>(nz, vt, static_cast<T*>(AT.val));
+        }
+        if (m) CK(cudaMemcpyAsync(P.Dr.data(), dr, size_t(m) * sizeof(double), cudaMemcpyDeviceToHost, st));
+        if (n) CK(cudaMemcpyAsync(P.Dc.data(), dc, size_t(n) * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        CK(cudaGetLastError());
+        }  // FP64 scratch released
+        t0 = Clock::now();
+        hA = Csr(), hAT = Csr();
+        scale_vectors(md, sign, P.Dr, P.Dc, P);
+        hs += since(t0);
+        if (host_s) *host_s = hs;
+        P.A = Csr(), P.AT = Csr();
+        P.A.rows = m, P.AT.rows = n;
+        finish_init(P.c.data(), P.l.data(), P.u.data(), P.rl.data(), P.ru.data(), P.Dr.data(), P.Dc.data());
+        nnz = nz;
+    }
+    void finish_init(const double* hc_ptr, const double* hl, const double* hu, const double* hrl_ptr,
+                     const double* hru_ptr, const double* hDr, const double* hDc) {
         c = upload(hc_ptr, n), l = upload(hl, n), u = upload(hu, n), Dc = upload(hDc, n);
         rl = upload(hrl_ptr, m), ru = upload(hru_ptr, m), Dr = upload(hDr, m);
         par = zeros<double>(2);
@@ -164,6 +248,7 @@ struct Engine final : EngineBase {
         CK(cudaMallocHost(&h_out, 32 * sizeof(double)));
         CK(cudaMallocHost(&h_flag, sizeof(int)));
         CK(cudaStreamSynchronize(st));
+        size_t free1, total;
         CK(cudaMemGetInfo(&free1, &total));
         mem_used = free0 - free1;
     }
@@ -384,6 +469,14 @@ void engine_init(EngineBase& e, int precision, const taral_csr& A, const taral_c
         static_cast<Engine<double>&>(e).init(A, AT, c, l, u, rl, ru, Dr, Dc, m, n, freq, flags);
 }
 
+void engine_init_model(EngineBase& e, int precision, const taral_model& md, double sign, Scaled& P, int freq,
+                       unsigned flags, double* host_s) {
+    if (precision == TARAL_FP32)
+        static_cast<Engine<float>&>(e).init_model(md, sign, P, freq, flags, host_s);
+    else
+        static_cast<Engine<double>&>(e).init_model(md, sign, P, freq, flags, host_s);
+}
+
 std::string cuda_error_message(const void* exc) { return static_cast<const CudaError*>(exc)->msg; }
 
 }  // namespace taral
@@ -445,6 +538,28 @@ extern "C" int pdhg_create(const taral_csr* A, const taral_csr* AT, const double
     try {
         ctx->e = taral::make_engine(precision);
         taral::engine_init(*ctx->e, precision, *A, *AT, c, l, u, rl, ru, Dr, Dc, m, n, eval_freq, flags);
+    } catch (const taral::CudaError& ex) {
+        std::string msg = ex.msg;
+        delete ctx;
+        return msg.find("cudaMalloc") != std::string::npos ? TARAL_ERR_ALLOC : TARAL_ERR_CUDA;
+    } catch (const std::bad_alloc&) {
+        delete ctx;
+        return TARAL_ERR_ALLOC;
+    }
+    *out = ctx;
+    return TARAL_OK;
+}
+
+int pdhg_create_model_ctx(const taral_model* md, int precision, int eval_freq, unsigned flags, taral::Scaled& P,
+                          pdhg_ctx** out) {
+    *out = nullptr;
+    int dev_count = 0;
+    if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0) return TARAL_ERR_NO_DEVICE;
+    auto* ctx = new pdhg_ctx;
+    ctx->precision = precision;
+    try {
+        ctx->e = taral::make_engine(precision);
+        taral::engine_init_model(*ctx->e, precision, *md, md->maximize ? -1.0 : 1.0, P, eval_freq, flags, nullptr);
     } catch (const taral::CudaError& ex) {
         std::string msg = ex.msg;
         delete ctx;

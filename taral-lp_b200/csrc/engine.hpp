@@ -16,6 +16,7 @@ struct EngineBase {
     std::string name;
     size_t mem_used = 0;
     int64_t launches = 0;
+    int64_t nnz = 0;  // nonzeros of A
     virtual ~EngineBase() = default;
     virtual double power_norm(int iters) = 0;
     virtual void set_steps(double tau, double sigma) = 0;
@@ -41,5 +42,18 @@ void engine_init(EngineBase& e, int precision, const taral_csr& A, const taral_c
                  const double* l, const double* u, const double* rl, const double* ru, const double* Dr,
                  const double* Dc, int m, int n, int eval_freq, unsigned flags);
 std::vector<int4> build_row_blocks(const int64_t* ptr, int rows);
+// Set-up from the column-wise model with the scaling done on the device, bit-identical to build_scaled(): P gets
+// Dr, Dc, the scaled vectors and the norms (its matrices stay empty); host_s: seconds of host work.
+struct Scaled;
+void engine_init_model(EngineBase& e, int precision, const taral_model& md, double sign, Scaled& P, int eval_freq,
+                       unsigned flags, double* host_s);
+
+}  // namespace taral
+
+// A pdhg_ctx built by engine_init_model (the C ABI's pdhg_create_model); P as for engine_init_model.
+int pdhg_create_model_ctx(const taral_model* md, int precision, int eval_freq, unsigned flags, taral::Scaled& P,
+                          pdhg_ctx** out);
+
+namespace taral {
 
 }  // namespace taral

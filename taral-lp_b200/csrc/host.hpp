@@ -46,6 +46,9 @@ struct Csr {
     taral_csr view(int cols) const { return {rows, cols, int64_t(val.size()), ptr.data(), idx.data(), val.data()}; }
 };
 Csr transpose(const Csr& a, int cols);  // gpu/pdhg.cu:55-70
+// transpose() of the CSR given by (ptr, idx, val) with the scatter on `threads` threads; identical output.
+Csr transpose_par(const int64_t* ptr, const int32_t* idx, const double* val, int rows, int cols, int threads);
+int host_threads();
 
 // Scaled problem (gpu/pdhg.cu:72-78): A_s = diag(Dr) A diag(Dc).
 struct Scaled {
@@ -60,6 +63,9 @@ Scaled build_scaled(const taral_model& md, double sign);  // gpu/pdhg.cu:80-133
 void scale_matrix(const taral_model& md, Scaled& P);
 void scale_vectors(const taral_model& md, double sign, const std::vector<double>& Dr, const std::vector<double>& Dc,
                    Scaled& P);
+// The unscaled A (the transpose of the column-wise model with explicit zeros dropped) and A^T (the transpose of A):
+// the structure and entry order scale_matrix() works on (gpu/pdhg.cu:80-90, 131), before any scaling.
+void model_matrices(const taral_model& md, Csr& A, Csr& AT, int threads = 0);  // threads <= 0: host_threads()
 
 struct Options {  // gpu/pdhg.cu:744-750
     double tol = 1e-4, time_limit = 3600;

@@ -2,6 +2,7 @@
 // FP64, single pass order identical to the reference so the scaled matrix is bit-identical to it.
 #include <algorithm>
 #include <cmath>
+#include <thread>
 
 #include "host.hpp"
 
@@ -22,6 +23,69 @@ Csr transpose(const Csr& a, int cols) {  // counting sort; rows of the output as
             t.idx[p] = i, t.val[p] = a.val[k];
         }
     return t;
+}
+
+// The same counting sort with the scatter split over threads by ranges of output rows: every thread reads the
+// whole input in order and writes only its own rows, so each output row is filled in the sequential order and the
+// result is identical to transpose().
+Csr transpose_par(const int64_t* ptr, const int32_t* idx, const double* val, int rows, int cols, int threads) {
+    Csr t;
+    t.rows = cols;
+    const int64_t nnz = ptr[rows] - ptr[0];
+    t.ptr.assign(size_t(cols) + 1, 0);
+    for (int64_t k = ptr[0]; k < ptr[rows]; ++k) t.ptr[size_t(idx[k]) + 1]++;
+    for (int j = 0; j < cols; ++j) t.ptr[j + 1] += t.ptr[j];
+    t.idx.resize(size_t(nnz));
+    t.val.resize(size_t(nnz));
+    threads = int(std::max<int64_t>(1, std::min<int64_t>(threads, nnz / 65536)));
+    std::vector<int> cut(size_t(threads) + 1, cols);  // output rows [cut[q], cut[q+1]) belong to thread q
+    cut[0] = 0;
+    for (int q = 1; q < threads; ++q)
+        cut[q] = int(std::lower_bound(t.ptr.begin(), t.ptr.end(), nnz * q / threads) - t.ptr.begin());
+    for (int q = 1; q <= threads; ++q) cut[q] = std::max(cut[q], cut[q - 1]);
+    auto work = [&](int q) {
+        const int lo = cut[q], hi = cut[q + 1];
+        if (lo >= hi) return;
+        std::vector<int64_t> pos(t.ptr.begin() + lo, t.ptr.begin() + hi);
+        for (int i = 0; i < rows; ++i)
+            for (int64_t k = ptr[i]; k < ptr[i + 1]; ++k) {
+                const int j = idx[k];
+                if (j < lo || j >= hi) continue;
+                const int64_t p = pos[j - lo]++;
+                t.idx[p] = i, t.val[p] = val[k];
+            }
+    };
+    std::vector<std::thread> pool;
+    for (int q = 1; q < threads; ++q) pool.emplace_back(work, q);
+    work(0);
+    for (auto& th : pool) th.join();
+    return t;
+}
+
+int host_threads() {
+    const unsigned h = std::thread::hardware_concurrency();
+    return int(std::max(1u, std::min(h, 16u)));
+}
+
+void model_matrices(const taral_model& md, Csr& A, Csr& AT, int threads) {
+    if (threads <= 0) threads = host_threads();
+    const int64_t k0 = md.col_ptr[0], k1 = md.col_ptr[md.n];
+    bool zeros = false;
+    for (int64_t k = k0; k < k1 && !zeros; ++k) zeros = md.val[k] == 0;
+    if (!zeros) {
+        A = transpose_par(md.col_ptr, md.row_idx, md.val, md.n, md.m, threads);
+    } else {  // drop explicit zeros first (the column-wise copy the reference builds)
+        Csr T;
+        T.rows = md.n;
+        T.ptr.assign(size_t(md.n) + 1, 0);
+        for (int j = 0; j < md.n; ++j) {
+            for (int64_t k = md.col_ptr[j]; k < md.col_ptr[j + 1]; ++k)
+                if (md.val[k] != 0) T.idx.push_back(md.row_idx[k]), T.val.push_back(md.val[k]);
+            T.ptr[j + 1] = int64_t(T.idx.size());
+        }
+        A = transpose_par(T.ptr.data(), T.idx.data(), T.val.data(), md.n, md.m, threads);
+    }
+    AT = transpose_par(A.ptr.data(), A.idx.data(), A.val.data(), md.m, md.n, threads);
 }
 
 void scale_matrix(const taral_model& md, Scaled& P) {

@@ -52,9 +52,7 @@ int solve_model(const taral_model& md, const Options& o, SolveResult& res, const
         return TARAL_ERR_INPUT;
     }
     auto t = Clock::now();
-    Scaled P = build_scaled(md, md.maximize ? -1.0 : 1.0);
-    res.scale_s = since(t);
-    t = Clock::now();
+    Scaled P;
     int dev_count = 0;
     if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0) {
         res.error = "no CUDA device";
@@ -69,9 +67,8 @@ int solve_model(const taral_model& md, const Options& o, SolveResult& res, const
     std::unique_ptr<EngineBase> e;
     try {
         e = make_engine(o.precision);
-        taral_csr A = P.A.view(P.n), AT = P.AT.view(P.m);
-        engine_init(*e, o.precision, A, AT, P.c.data(), P.l.data(), P.u.data(), P.rl.data(), P.ru.data(),
-                    P.Dr.data(), P.Dc.data(), P.m, P.n, o.eval_freq, o.graph ? 0u : TARAL_FLAG_NO_GRAPH);
+        engine_init_model(*e, o.precision, md, md.maximize ? -1.0 : 1.0, P, o.eval_freq,
+                          o.graph ? 0u : TARAL_FLAG_NO_GRAPH, &res.scale_s);
     } catch (const std::bad_alloc&) {
         res.error = "host allocation failed";
         return TARAL_ERR_ALLOC;
@@ -82,7 +79,7 @@ int solve_model(const taral_model& md, const Options& o, SolveResult& res, const
         res.error = "device initialisation failed (out of device memory?)";
         return TARAL_ERR_ALLOC;
     }
-    res.transfer_s = since(t);
+    res.transfer_s = since(t) - res.scale_s;  // upload, device scaling and narrowing
     res.device_mem_bytes = e->mem_used;
     res.device_name = e->name;
     // Warm start in the original space -> scaled space: x_s = x / Dc, z_s = y / Dr.
@@ -110,7 +107,7 @@ int solve_model(const taral_model& md, const Options& o, SolveResult& res, const
     res.solve_s = since(t);
     res.kernel_launches = e->launches;
     res.fin = finish_point(md, P, res.outcome);
-    res.nnz = int64_t(P.A.val.size());
+    res.nnz = e->nnz;
     res.m = P.m, res.n = P.n;
     return TARAL_OK;
 }
@@ -170,15 +167,9 @@ extern "C" int pdhg_create_model(const taral_model* md, int precision, int eval_
     *out = nullptr;
     if (taral::input_error(*md)) return TARAL_ERR_UNSUPPORTED;
     if (!taral::check_model(*md).empty()) return TARAL_ERR_INPUT;
+    if (precision != TARAL_FP64 && precision != TARAL_FP32) return TARAL_ERR_INPUT;
     taral::Scaled P;
-    try {
-        P = taral::build_scaled(*md, md->maximize ? -1.0 : 1.0);
-    } catch (const std::bad_alloc&) {
-        return TARAL_ERR_ALLOC;
-    }
-    taral_csr A = P.A.view(P.n), AT = P.AT.view(P.m);
-    int rc = pdhg_create(&A, &AT, P.c.data(), P.l.data(), P.u.data(), P.rl.data(), P.ru.data(), P.Dr.data(),
-                         P.Dc.data(), P.m, P.n, precision, eval_freq, flags, out);
+    int rc = pdhg_create_model_ctx(md, precision, eval_freq, flags, P, out);
     if (rc == TARAL_OK) {
         if (bnorm) *bnorm = P.bnorm;
         if (cnorm) *cnorm = P.cnorm;
