@@ -1,4 +1,5 @@
-"""Build the engine in-tree: lib/libtaral_pdhg.so (CUDA kernels for sm_100a + host code + C ABI) and bin/pdhg.
+"""Build the engine in-tree: lib/libtaral_pdhg.so (CUDA kernels for sm_100a + host code + C ABI), bin/pdhg (the
+CLI) and bin/gather_probe (the random-gather floor measurement of the SpMV phases).
 
 nvcc cross-compiles without a GPU. Objects are rebuilt only when a source or header is newer.
 Usage: python taral-lp_b200/build.py [--force]
@@ -17,6 +18,7 @@ CSRC = PKG / "csrc"
 OBJ = PKG / "_build"
 LIB = PKG / "lib" / "libtaral_pdhg.so"
 CLI = PKG / "bin" / "pdhg"
+PROBE = PKG / "bin" / "gather_probe"
 NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-O3", "-I", str(ROOT / "include")]
@@ -56,6 +58,9 @@ def build(force: bool = False) -> Path:
     if force or _stale(CLI, [cli_o, LIB]):
         subprocess.run([NVCC, *ARCH, "-o", str(CLI), str(cli_o), "-L", str(LIB.parent), "-ltaral_pdhg",
                         "-Xlinker", "-rpath,$ORIGIN/../lib"], check=True)
+    probe_src = CSRC / "gather_probe.cu"
+    if force or _stale(PROBE, [probe_src]):
+        subprocess.run([NVCC, *ARCH, "-O3", "-std=c++17", "-o", str(PROBE), str(probe_src)], check=True)
     return LIB
 
 

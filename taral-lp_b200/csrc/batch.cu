@@ -14,8 +14,10 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <map>
+#include <tuple>
 #include <memory>
 #include <string>
 #include <thread>
@@ -25,6 +27,7 @@
 #include "engine.hpp"
 #include "host.hpp"
 #include "kernels.cuh"
+#include "scaling.cuh"
 #include "solve.hpp"
 
 namespace taral {
@@ -50,72 +53,339 @@ __device__ __forceinline__ double dmax(double a, double b) { return a < b ? b : 
 __device__ __forceinline__ double dmin(double a, double b) { return b < a ? b : a; }  // std::min semantics
 
 // ---------------------------------------------------------------------------------------------- batch kernels
-// Per-block partial sums of the row (ROW = true) or column KKT scalars, blocks in evaluation order.
-// Row part (gpu/pdhg.cu:236-251), column part (:253-271); f per instance (1 for the current point).
-template <class T, class V, bool ROW>
-__global__ void __launch_bounds__(kThreads) k_eval_blocks(const int4* __restrict__ blk, const int4* __restrict__ ext,
-                                                          const int* __restrict__ active, const double* __restrict__ fi,
-                                                          const V* __restrict__ a, const V* __restrict__ b,
-                                                          const T* __restrict__ lo_v, const T* __restrict__ up_v,
-                                                          const T* __restrict__ c_v, const T* __restrict__ D,
-                                                          const T* __restrict__ last, double* part) {
-    const int4 e4 = ext[blockIdx.x];
-    if (!active[e4.x]) return;
-    const int4 meta = blk[blockIdx.x];
-    const int nrows = meta.y & 0xffff, r = meta.x + e4.y + threadIdx.x;
-    const double f = fi ? fi[e4.x] : 1.0;
-    double v[5] = {0, 0, 0, 0, 0};
-    if (int(threadIdx.x) < nrows) {
-        if (ROW) {  // a = Ax (or A xs), b = z (or zs)
-            double ax = double(a[r]) * f, zz = double(b[r]) * f, lo = lo_v[r], up = up_v[r];
-            double res = ax < lo ? lo - ax : (ax > up ? ax - up : 0), ro = res / double(D[r]);
-            double rr = ro * row_rel_weight(lo, up, double(D[r]));
-            v[0] = res * res, v[1] = ro * ro, v[2] = rr * rr;
-            if (zz > 0 && up < INFINITY) v[3] -= zz * up;
-            if (zz < 0 && lo > -INFINITY) v[3] -= zz * lo;
-            double dz = zz - double(last[r]);
-            v[4] = dz * dz;
-        } else {  // a = x (or xs), b = ATz (or A^T zs); c_v = c, lo_v = l, up_v = u
-            double xx = double(a[r]) * f, cj = c_v[r], d = cj + double(b[r]) * f, lo = lo_v[r], up = up_v[r], res = 0;
-            v[2] = cj * xx;
-            if (d > 0) {
-                if (lo > -INFINITY) v[3] = d * lo;
-                else res = d;
-            } else if (d < 0) {
-                if (up < INFINITY) v[3] = d * up;
-                else res = -d;
+// ---------------------------------------------------------------------------------------------- pack layout
+// Instances that share one constraint matrix are grouped in PACKS of W in {1, 2, 4, 8} slots. Every per-instance
+// vector stores the entry of (slot t, row r) of a pack at base + r * W + t: the W instances' entries of one row (or
+// column) are adjacent. One CTA takes one row block of the shared matrix for all W slots of a pack: the block's
+// column indices and values are staged in shared memory once, and lane (row, slot) gathers x at gbase + col * W +
+// slot, so the W slots of a column share one memory segment -- a gathered 32-byte sector serves up to 8 instances
+// instead of one, and the matrix block is read once for the pack.
+// Per slot, every row is summed in exactly the order of the single-instance skeleton (block_sums: products rounded
+// to the product type, FP64 sums; a thread per row up to kShort nonzeros, a warp per longer row, the whole CTA for a
+// row longer than kTile), so a batched instance follows the same iterates as the same instance solved alone.
+// Per CTA: blk = {first row in the concatenated row pointers, rows, first nonzero, end}; ext = {pack, vector index
+// of (first row, slot 0), gather base of the pack's other-side vector, W}. slot_inst[8 pack + t]: the instance in
+// slot t, or -1 for an unused slot.
+// Row blocks of a pack of width W hold at most pack_tile(W) nonzeros and kRowsMax / W rows, so that the block's
+// (nonzero, slot) pairs fit the kTile-product staging of the single-instance skeleton: (tile + 3) W < kTile + 4.
+__host__ __device__ constexpr int pack_tile(int W) { return (kTile + 4) / W - 4; }
+constexpr int kPairs = (kTile + 4 + kThreads - 1) / kThreads;  // staged pairs per thread (8)
+static_assert((pack_tile(8) + 3) * 8 <= kPairs * kThreads && (pack_tile(1) + 3) <= kPairs * kThreads, "pairs");
+
+__device__ __forceinline__ int log2w(int W) { return W >= 8 ? 3 : W >= 4 ? 2 : W >= 2 ? 1 : 0; }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+
+template <class P>
+struct PackSmem {
+    P prod[kPairs * kThreads + kPairs * kThreads / 32];  // pair q = (nonzero - a0) * W + slot at pidx(q)
+    double rowsum[kRowsMax];                              // per (row, slot) item
+    int rptr[kRowsMax + 1];
+    short longq[kRowsMax];
+    int nlong;
+    double part[kThreads / 32];
+};
+
+template <class T, class X, class E>
+__global__ void __launch_bounds__(kThreads, 6) k_pack_spmv(const int* __restrict__ ptr,
+                                                                     const int* __restrict__ idx,
+                                                                     const T* __restrict__ val,
+                                                                     const X* __restrict__ xin,
+                                                                     const int4* __restrict__ blk,
+                                                                     const int4* __restrict__ ext,
+                                                                     const int* __restrict__ slot_inst,
+                                                                     const int* __restrict__ active, E epi) {
+    using P = typename ProdT<T, X>::type;
+    __shared__ PackSmem<P> sm;
+    const int4 e4 = __ldg(ext + blockIdx.x);
+    const int pack = e4.x, vbase = e4.y, gbase = e4.z, W = e4.w, lw = log2w(W);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, my_t = tid & (W - 1);
+    const int my_inst = slot_inst[8 * pack + my_t];
+    const bool my_live = my_inst >= 0 && active[my_inst] != 0;
+    if (!__syncthreads_or(my_live)) return;
+    const int4 meta = __ldg(blk + blockIdx.x);
+    const int r0 = meta.x, nrows = meta.y & 0xffff, p0 = meta.z, p1 = meta.w, len = p1 - p0;
+    if (len > pack_tile(W)) {  // one long row: per live slot, the whole CTA (block_sums' long-row order)
+        const int a0 = p0 & ~3;
+        for (int t = 0; t < W; ++t) {
+            const int inst = slot_inst[8 * pack + t];
+            if (inst < 0 || !active[inst]) continue;  // uniform over the CTA
+            double s = 0;
+            for (int q = a0 + 4 * tid; q < p1; q += 4 * kThreads)
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const int k = q + e;
+                    if (k >= p0 && k < p1) s += double(__ldg(val + k)) * double(__ldg(xin + gbase + __ldg(idx + k) * W + t));
+                }
+            for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
+            if (lane == 0) sm.part[warp] = s;
+            __syncthreads();
+            if (tid == 0) {
+                double tot = 0;
+                for (int w = 0; w < kThreads / 32; ++w) tot += sm.part[w];
+                const int o = vbase + t;
+                const auto ops = epi.load(o, inst);
+                epi.apply(o, tot, ops);
             }
-            double ro = res / double(D[r]), dx = xx - double(last[r]);
-            v[0] = res * res, v[1] = ro * ro, v[4] = dx * dx;
+            __syncthreads();
+        }
+        return;
+    }
+    // item tid = (row tid >> lw, slot my_t): its epilogue operands are fetched before the matrix stream
+    const bool mine = my_live && tid < (nrows << lw);
+    typename E::Ops ops{};
+    if (mine) ops = epi.load(vbase + tid, my_inst);
+    // 1. stage the products of the block's (nonzero, slot) pairs: all index / value loads, then all gathers
+    const int a0 = p0 & ~3, npairs = (p1 - a0) << lw;
+    int c[kPairs];
+    T v[kPairs];
+#pragma unroll
+    for (int i = 0; i < kPairs; ++i) {
+        const int q = tid + i * kThreads, k = a0 + (q >> lw);
+        const bool in = my_live && q < npairs && k >= p0;
+        c[i] = in ? __ldg(idx + k) : -1;
+        v[i] = in ? __ldg(val + k) : T(0);
+    }
+    X g[kPairs];
+#pragma unroll
+    for (int i = 0; i < kPairs; ++i) g[i] = c[i] >= 0 ? gather(xin + gbase + c[i] * W + my_t) : X(0);
+#pragma unroll
+    for (int i = 0; i < kPairs; ++i)
+        if (c[i] >= 0) sm.prod[pidx(tid + i * kThreads)] = mul_rn(P(v[i]), P(g[i]));
+    for (int t = tid; t <= nrows; t += kThreads) sm.rptr[t] = ptr[r0 + t] - a0;
+    if (tid == 0) sm.nlong = 0;
+    __syncthreads();
+    // 2. sums: an item of at most kShort nonzeros by its own thread, longer ones by a warp each
+    if (mine) {
+        const int rl = tid >> lw, a = sm.rptr[rl], b = sm.rptr[rl + 1];
+        if (b - a <= kShort) {
+            double s = 0;
+            int k = a;
+            for (; k + 8 <= b; k += 8) {  // eight loads in flight, then the adds in entry order
+                P t[8];
+#pragma unroll
+                for (int e = 0; e < 8; ++e) t[e] = sm.prod[pidx(((k + e) << lw) + my_t)];
+#pragma unroll
+                for (int e = 0; e < 8; ++e) s += double(t[e]);
+            }
+            for (; k < b; ++k) s += double(sm.prod[pidx((k << lw) + my_t)]);
+            sm.rowsum[tid] = s;
+        } else {
+            sm.longq[atomicAdd(&sm.nlong, 1)] = short(tid);
         }
     }
-    __shared__ double sh[5][kThreads / 32];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-#pragma unroll
-    for (int k = 0; k < 5; ++k) {
-        double s = v[k];
-        for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
-        if (lane == 0) sh[k][w] = s;
+    __syncthreads();
+    for (int i = warp; i < sm.nlong; i += kThreads / 32) {  // warp-uniform trip count: all lanes shuffle
+        const int q = sm.longq[i], rl = q >> lw, t = q & (W - 1);
+        double s = 0;
+        for (int k = sm.rptr[rl] + lane; k < sm.rptr[rl + 1]; k += 32) s += double(sm.prod[pidx((k << lw) + t)]);
+        for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+        if (lane == 0) sm.rowsum[q] = s;
     }
     __syncthreads();
-    if (threadIdx.x < 5) {
-        double s = 0;
-        for (int i = 0; i < kThreads / 32; ++i) s += sh[threadIdx.x][i];
-        part[size_t(blockIdx.x) * 5 + threadIdx.x] = s;
+    if (mine) epi.apply(vbase + tid, sm.rowsum[tid], ops);
+}
+
+// ---------------------------------------------------------------------------------------------- instance groups
+// Width-1 packs that share a matrix form GROUPS of up to kGroup instances. One CTA takes one row block of the shared
+// matrix for a whole group: the block's column indices and values are staged in shared memory once (16-byte loads),
+// then for each live instance in turn the CTA runs block_sums' sequence from the staged copy -- every thread's
+// gathers, the products into shared memory, a thread per row up to kShort nonzeros and a warp per longer row, the
+// fused epilogue -- so each instance gets exactly the single-instance kernel's sums, and the matrix block crosses
+// from L2 once per group instead of once per instance.
+// gext[kGroup * group + t] = {instance, row shift, gather offset, 0} of member t (instance -1: unused slot).
+constexpr int kGroup = 16;
+
+template <class T>
+struct GroupSmem {
+    int idx[kTile + 4];
+    T val[kTile + 4];
+};
+
+template <class T, class X, class E>
+__global__ void __launch_bounds__(kThreads, 6) k_group_spmv(const int* __restrict__ ptr, const int* __restrict__ idx,
+                                                           const T* __restrict__ val, const X* __restrict__ xin,
+                                                           const int4* __restrict__ blk, const int* __restrict__ grp,
+                                                           const int4* __restrict__ gext,
+                                                           const int* __restrict__ active, E epi) {
+    using P = typename ProdT<T, X>::type;
+    __shared__ RowSmem<P> sm;
+    __shared__ GroupSmem<T> gs;
+    const int g = __ldg(grp + blockIdx.x), tid = threadIdx.x;
+    int live_mask = 0;
+    for (int t = 0; t < kGroup; ++t) {
+        const int inst = __ldg(&gext[kGroup * g + t].x);
+        if (inst >= 0 && active[inst]) live_mask |= 1 << t;
+    }
+    if (!live_mask) return;  // uniform: every thread reads the same flags
+    const int4 meta = __ldg(blk + blockIdx.x);
+    const int r0 = meta.x, nrows = meta.y & 0xffff, p0 = meta.z, p1 = meta.w, len = p1 - p0;
+    const bool mine = tid < nrows;
+    if (len > kTile) {  // one long row: block_sums reads it from global memory for each instance
+        for (int t = 0; t < kGroup; ++t) {
+            if (!(live_mask >> t & 1)) continue;
+            const int4 e4 = __ldg(gext + kGroup * g + t);
+            typename E::Ops ops{};
+            if (mine) ops = epi.load(r0 + e4.y + tid, e4.x);
+            block_sums<T, X, true>(ptr, idx, val, xin + e4.z, meta, sm);
+            if (mine) epi.apply(r0 + e4.y + tid, sm.rowsum[tid], ops);
+            __syncthreads();
+        }
+        return;
+    }
+    // stage the block: quads from a0 = p0 & ~3, entry k at k - a0
+    const int a0 = p0 & ~3;
+    for (int q = a0 + 4 * tid; q < p1; q += 4 * kThreads) {
+        if (q >= p0 && q + 4 <= p1) {
+            T v[4];
+            int c[4];
+            Quad<T>::load(val + q, v), load_idx4(idx + q, c);
+#pragma unroll
+            for (int e = 0; e < 4; ++e) gs.val[q - a0 + e] = v[e], gs.idx[q - a0 + e] = c[e];
+        } else {
+#pragma unroll
+            for (int e = 0; e < 4; ++e)
+                if (q + e >= p0 && q + e < p1) gs.val[q - a0 + e] = __ldg(val + q + e), gs.idx[q - a0 + e] = __ldg(idx + q + e);
+        }
+    }
+    for (int t = tid; t <= nrows; t += kThreads) sm.rptr[t] = ptr[r0 + t] - p0;
+    __syncthreads();
+    const int lane = tid & 31, warp = tid >> 5;
+    for (int t = 0; t < kGroup; ++t) {
+        if (!(live_mask >> t & 1)) continue;
+        const int4 e4 = __ldg(gext + kGroup * g + t);
+        const X* xg = xin + e4.z;
+        typename E::Ops ops{};
+        if (mine) ops = epi.load(r0 + e4.y + tid, e4.x);
+        if (tid == 0) sm.nlong = 0;
+        // products: the same (thread, quad) assignment and rounding as block_sums
+        X gv[kQuads][4];
+        int c[kQuads][4];
+#pragma unroll
+        for (int i = 0; i < kQuads; ++i) {
+            const int q = a0 + 4 * (tid + i * kThreads);
+#pragma unroll
+            for (int e = 0; e < 4; ++e) c[i][e] = (q + e >= p0 && q + e < p1) ? gs.idx[q + e - a0] : -1;
+        }
+#pragma unroll
+        for (int i = 0; i < kQuads; ++i)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) gv[i][e] = c[i][e] >= 0 ? gather(xg + c[i][e]) : X(0);
+#pragma unroll
+        for (int i = 0; i < kQuads; ++i) {
+            const int q = a0 + 4 * (tid + i * kThreads);
+#pragma unroll
+            for (int e = 0; e < 4; ++e)
+                if (c[i][e] >= 0) sm.prod[pidx(q + e - p0)] = P(gs.val[q + e - a0]) * P(gv[i][e]);
+        }
+        __syncthreads();
+        if (mine) {
+            const int a = sm.rptr[tid], b = sm.rptr[tid + 1];
+            if (b - a <= kShort) {
+                double s = 0;
+                int k = a;
+                for (; k + 4 <= b; k += 4) {
+                    P tt[4];
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) tt[e] = sm.prod[pidx(k + e)];
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) s += double(tt[e]);
+                }
+                for (; k < b; ++k) s += double(sm.prod[pidx(k)]);
+                sm.rowsum[tid] = s;
+            } else {
+                sm.longrow[atomicAdd(&sm.nlong, 1)] = short(tid);
+            }
+        }
+        __syncthreads();
+        for (int i = warp; i < sm.nlong; i += kThreads / 32) {
+            const int r = sm.longrow[i];
+            double s = 0;
+            for (int k = sm.rptr[r] + lane; k < sm.rptr[r + 1]; k += 32) s += double(sm.prod[pidx(k)]);
+            for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+            if (lane == 0) sm.rowsum[r] = s;
+        }
+        __syncthreads();
+        if (mine) epi.apply(r0 + e4.y + tid, sm.rowsum[tid], ops);
+        __syncthreads();  // the next member reuses the product and row-sum arrays
     }
 }
 
-// One warp per instance: kkt[inst*10 + k] = sum of its blocks' partials, in block order (deterministic).
-__global__ void k_eval_finish(int ninst, const int* __restrict__ rr, const int* __restrict__ cr,
-                              const double* __restrict__ prow, const double* __restrict__ pcol,
-                              const int* __restrict__ active, double* kkt) {
+// Per-(CTA, slot) partial sums of the row (ROW = true) or column KKT scalars over one pack block, CTAs in
+// evaluation order (gpu/pdhg.cu:236-251 and :253-271); f per instance (1 for the current point).
+// part[(cta * 8 + slot) * 5 + k].
+template <class T, class V, bool ROW>
+__global__ void __launch_bounds__(kThreads) k_pack_eval(const int4* __restrict__ blk, const int4* __restrict__ ext,
+                                                         const int* __restrict__ slot_inst,
+                                                         const int* __restrict__ active, const double* __restrict__ fi,
+                                                         const V* __restrict__ a, const V* __restrict__ b,
+                                                         const T* __restrict__ lo_v, const T* __restrict__ up_v,
+                                                         const T* __restrict__ c_v, const T* __restrict__ D,
+                                                         const T* __restrict__ last, double* part) {
+    const int4 e4 = ext[blockIdx.x];
+    const int pack = e4.x, vbase = e4.y, W = e4.w, lw = log2w(W);
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5, my_t = tid & (W - 1);
+    const int inst = slot_inst[8 * pack + my_t];
+    const bool live = inst >= 0 && active[inst] != 0;
+    const int nrows = blk[blockIdx.x].y & 0xffff;
+    const double f = live && fi ? fi[inst] : 1.0;
+    double v[5] = {0, 0, 0, 0, 0};
+    if (live)
+        for (int q = tid; q < (nrows << lw); q += kThreads) {
+            const int r = vbase + q;
+            if (ROW) {  // a = Ax (or A xs), b = z (or zs)
+                double ax = double(a[r]) * f, zz = double(b[r]) * f, lo = lo_v[r], up = up_v[r];
+                double res = ax < lo ? lo - ax : (ax > up ? ax - up : 0), ro = res / double(D[r]);
+                double rr = ro * row_rel_weight(lo, up, double(D[r]));
+                v[0] += res * res, v[1] += ro * ro, v[2] += rr * rr;
+                if (zz > 0 && up < INFINITY) v[3] -= zz * up;
+                if (zz < 0 && lo > -INFINITY) v[3] -= zz * lo;
+                double dz = zz - double(last[r]);
+                v[4] += dz * dz;
+            } else {  // a = x (or xs), b = ATz (or A^T zs); c_v = c, lo_v = l, up_v = u
+                double xx = double(a[r]) * f, cj = c_v[r], d = cj + double(b[r]) * f, lo = lo_v[r], up = up_v[r],
+                       res = 0;
+                v[2] += cj * xx;
+                if (d > 0) {
+                    if (lo > -INFINITY) v[3] += d * lo;
+                    else res = d;
+                } else if (d < 0) {
+                    if (up < INFINITY) v[3] += d * up;
+                    else res = -d;
+                }
+                double ro = res / double(D[r]), dx = xx - double(last[r]);
+                v[0] += res * res, v[1] += ro * ro, v[4] += dx * dx;
+            }
+        }
+    __shared__ double sh[kThreads / 32][8][5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        double s = v[k];
+        for (int off = 16; off >= W; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);  // lanes of one slot
+        if (lane < W) sh[w][lane][k] = s;
+    }
+    __syncthreads();
+    if (tid < 8 * 5) {
+        const int t = tid / 5, k = tid % 5;
+        double s = 0;
+        if (t < W)
+            for (int i = 0; i < kThreads / 32; ++i) s += sh[i][t][k];
+        part[(size_t(blockIdx.x) * 8 + t) * 5 + k] = s;
+    }
+}
+
+// One warp per instance: kkt[inst*10 + k] = sum of its pack blocks' partials, in block order (deterministic).
+__global__ void k_eval_finish(int ninst, const int2* __restrict__ where, const int* __restrict__ rr,
+                              const int* __restrict__ cr, const double* __restrict__ prow,
+                              const double* __restrict__ pcol, const int* __restrict__ active, double* kkt) {
     const int inst = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
     if (inst >= ninst || !active[inst] || lane >= 10) return;
+    const int2 pt = where[inst];  // {pack, slot}
     double s = 0;
     if (lane < 5)
-        for (int b = rr[inst]; b < rr[inst + 1]; ++b) s += prow[size_t(b) * 5 + lane];
+        for (int b = rr[pt.x]; b < rr[pt.x + 1]; ++b) s += prow[(size_t(b) * 8 + pt.y) * 5 + lane];
     else
-        for (int b = cr[inst]; b < cr[inst + 1]; ++b) s += pcol[size_t(b) * 5 + lane - 5];
+        for (int b = cr[pt.x]; b < cr[pt.x + 1]; ++b) s += pcol[(size_t(b) * 8 + pt.y) * 5 + lane - 5];
     kkt[inst * 10 + lane] = s;
 }
 
@@ -192,68 +462,80 @@ __global__ void k_gather_f(int ninst, const InstState* st, double* f) {
     if (i < ninst) f[i] = st[i].f;
 }
 
-// First primal step of the block for every running instance, over column blocks (rows of A^T).
+// Elementwise work over the live (row, slot) entries of one pack block per CTA (evaluation-order block lists).
+#define PACK_ENTRIES(ACTIVE_EXPR)                                                                   \
+    const int4 e4 = ext[blockIdx.x];                                                                \
+    const int pack = e4.x, vbase = e4.y, W = e4.w, lw = log2w(W);                                   \
+    const int my_t = threadIdx.x & (W - 1), inst = slot_inst[8 * pack + my_t];                      \
+    const int nrows = blk[blockIdx.x].y & 0xffff;                                                   \
+    const bool live = inst >= 0 && (ACTIVE_EXPR);
+
+// First primal step of the block for every running instance (gpu/pdhg.cu:208-214).
 template <class T>
-__global__ void k_xupd_blocks(const int4* __restrict__ blk, const int4* __restrict__ ext, const int* __restrict__ active,
-                              T* __restrict__ x, const T* __restrict__ ATz, const T* __restrict__ c,
-                              const T* __restrict__ l, const T* __restrict__ u, const double* __restrict__ par,
-                              double* __restrict__ xs) {
-    const int4 e4 = ext[blockIdx.x];
-    if (!active[e4.x]) return;
-    const int4 meta = blk[blockIdx.x];
-    const int nrows = meta.y & 0xffff;
-    if (int(threadIdx.x) >= nrows) return;
-    const int j = meta.x + e4.y + threadIdx.x;
-    const T xn = T(clampv(double(x[j]) - par[2 * e4.x] * (double(c[j]) + double(ATz[j])), double(l[j]), double(u[j])));
-    x[j] = xn, xs[j] += double(xn);
+__global__ void k_pack_xupd(const int4* __restrict__ blk, const int4* __restrict__ ext,
+                            const int* __restrict__ slot_inst, const int* __restrict__ active, T* __restrict__ x,
+                            const T* __restrict__ ATz, const T* __restrict__ c, const T* __restrict__ l,
+                            const T* __restrict__ u, const double* __restrict__ par, double* __restrict__ xs) {
+    PACK_ENTRIES(active[inst] != 0)
+    if (!live) return;
+    const double tau = par[2 * inst];
+    for (int q = threadIdx.x; q < (nrows << lw); q += blockDim.x) {
+        const int j = vbase + q;
+        const T xn = T(clampv(double(x[j]) - tau * (double(c[j]) + double(ATz[j])), double(l[j]), double(u[j])));
+        x[j] = xn, xs[j] += double(xn);
+    }
 }
 
 // Restart of the flagged instances (gpu/pdhg.cu:293-299): flag 2 -> average * f, 1 -> current point.
 template <class T>
-__global__ void k_restart_blocks(const int4* __restrict__ blk, const int4* __restrict__ ext, const int* __restrict__ flag,
-                                 const InstState* __restrict__ st, T* __restrict__ x, double* __restrict__ xs,
-                                 T* __restrict__ xlast) {
-    const int4 e4 = ext[blockIdx.x];
-    const int fl = flag[e4.x];
-    if (!fl) return;
-    const int4 meta = blk[blockIdx.x];
-    const int nrows = meta.y & 0xffff;
-    if (int(threadIdx.x) >= nrows) return;
-    const int j = meta.x + e4.y + threadIdx.x;
-    T v = fl == 2 ? T(xs[j] * st[e4.x].f_restart) : x[j];
-    x[j] = v, xlast[j] = v, xs[j] = 0;
+__global__ void k_pack_restart(const int4* __restrict__ blk, const int4* __restrict__ ext,
+                               const int* __restrict__ slot_inst, const int* __restrict__ flag,
+                               const InstState* __restrict__ st, T* __restrict__ x, double* __restrict__ xs,
+                               T* __restrict__ xlast) {
+    PACK_ENTRIES(flag[inst] != 0)
+    if (!live) return;
+    const int fl = flag[inst];
+    const double fr = st[inst].f_restart;
+    for (int q = threadIdx.x; q < (nrows << lw); q += blockDim.x) {
+        const int j = vbase + q;
+        const T v = fl == 2 ? T(xs[j] * fr) : x[j];
+        x[j] = v, xlast[j] = v, xs[j] = 0;
+    }
 }
 
-// Per-instance power-iteration step over column blocks: partial ||v||^2, then one thread per instance.
+// Power iteration: per-(CTA, slot) partial ||v||^2 over one pack block (part[cta * 8 + slot]).
 template <class T>
-__global__ void k_pow_part(const int4* __restrict__ blk, const int4* __restrict__ ext, const int* __restrict__ active,
-                           const T* __restrict__ v, double* part) {
-    const int4 e4 = ext[blockIdx.x];
-    if (!active[e4.x]) return;
-    const int4 meta = blk[blockIdx.x];
-    const int nrows = meta.y & 0xffff;
+__global__ void __launch_bounds__(kThreads) k_pack_pow_part(const int4* __restrict__ blk, const int4* __restrict__ ext,
+                                                             const int* __restrict__ slot_inst,
+                                                             const int* __restrict__ active, const T* __restrict__ v,
+                                                             double* part) {
+    PACK_ENTRIES(active[inst] != 0)
     double a = 0;
-    if (int(threadIdx.x) < nrows) {
-        double t = double(v[meta.x + e4.y + threadIdx.x]);
-        a = t * t;
-    }
-    for (int off = 16; off > 0; off >>= 1) a += __shfl_down_sync(0xffffffffu, a, off);
-    __shared__ double sh[kThreads / 32];
-    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = a;
+    if (live)
+        for (int q = threadIdx.x; q < (nrows << lw); q += kThreads) {
+            const double t = double(v[vbase + q]);
+            a += t * t;
+        }
+    for (int off = 16; off >= W; off >>= 1) a += __shfl_xor_sync(0xffffffffu, a, off);
+    __shared__ double sh[kThreads / 32][8];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane < W) sh[w][lane] = a;
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (threadIdx.x < 8) {
         double s = 0;
-        for (int i = 0; i < kThreads / 32; ++i) s += sh[i];
-        part[blockIdx.x] = s;
+        if (int(threadIdx.x) < W)
+            for (int i = 0; i < kThreads / 32; ++i) s += sh[i][threadIdx.x];
+        part[size_t(blockIdx.x) * 8 + threadIdx.x] = s;
     }
 }
 
-__global__ void k_pow_update(int ninst, const int* __restrict__ cr, const double* __restrict__ part, double* est,
-                             double* scale, int* active, int it) {
+__global__ void k_pow_update(int ninst, const int2* __restrict__ where, const int* __restrict__ cr,
+                             const double* __restrict__ part, double* est, double* scale, int* active, int it) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= ninst || !active[i]) return;
+    const int2 pt = where[i];
     double s = 0;
-    for (int b = cr[i]; b < cr[i + 1]; ++b) s += part[b];
+    for (int b = cr[pt.x]; b < cr[pt.x + 1]; ++b) s += part[size_t(b) * 8 + pt.y];
     double prev = est[i];
     if (s <= 0) {
         est[i] = 0, active[i] = 0;
@@ -265,27 +547,30 @@ __global__ void k_pow_update(int ninst, const int* __restrict__ cr, const double
 }
 
 template <class T>
-__global__ void k_pow_scale(const int4* __restrict__ blk, const int4* __restrict__ ext, const int* __restrict__ active,
-                            const double* __restrict__ scale, T* __restrict__ v) {
-    const int4 e4 = ext[blockIdx.x];
-    if (!active[e4.x]) return;
-    const int4 meta = blk[blockIdx.x];
-    if (int(threadIdx.x) >= (meta.y & 0xffff)) return;
-    const int j = meta.x + e4.y + threadIdx.x;
-    v[j] = T(double(v[j]) * scale[e4.x]);
+__global__ void k_pack_pow_scale(const int4* __restrict__ blk, const int4* __restrict__ ext,
+                                 const int* __restrict__ slot_inst, const int* __restrict__ active,
+                                 const double* __restrict__ scale, T* __restrict__ v) {
+    PACK_ENTRIES(active[inst] != 0)
+    if (!live) return;
+    const double sc = scale[inst];
+    for (int q = threadIdx.x; q < (nrows << lw); q += blockDim.x) v[vbase + q] = T(double(v[vbase + q]) * sc);
 }
 
-// Download: out = (avg ? sum * f : point) for each instance's range.
+// Download: out = (avg ? sum * f : point) for every used slot.
 template <class T>
-__global__ void k_out_blocks(const int4* __restrict__ blk, const int4* __restrict__ ext, const InstState* __restrict__ st,
-                             const T* __restrict__ x, const double* __restrict__ xs, double* __restrict__ out) {
-    const int4 e4 = ext[blockIdx.x];
-    const int4 meta = blk[blockIdx.x];
-    if (int(threadIdx.x) >= (meta.y & 0xffff)) return;
-    const int j = meta.x + e4.y + threadIdx.x;
-    const InstState& s = st[e4.x];
-    out[j] = s.avg_final ? xs[j] * (1.0 / double(s.n_since > 1 ? s.n_since : 1)) : double(x[j]);
+__global__ void k_pack_out(const int4* __restrict__ blk, const int4* __restrict__ ext,
+                           const int* __restrict__ slot_inst, const InstState* __restrict__ st,
+                           const T* __restrict__ x, const double* __restrict__ xs, double* __restrict__ out) {
+    PACK_ENTRIES(true)
+    if (!live) return;
+    const InstState& s = st[inst];
+    const double f = 1.0 / double(s.n_since > 1 ? s.n_since : 1);
+    for (int q = threadIdx.x; q < (nrows << lw); q += blockDim.x) {
+        const int j = vbase + q;
+        out[j] = s.avg_final ? xs[j] * f : double(x[j]);
+    }
 }
+#undef PACK_ENTRIES
 
 __global__ void k_kkt_init(int ninst, InstState* st, const double* __restrict__ kc) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -312,15 +597,22 @@ __global__ void k_count(int ninst, const int* __restrict__ running, int* count) 
 
 // ---------------------------------------------------------------------------------------------- host side
 struct Shared {  // one distinct scaled matrix
-    Scaled S;    // matrix part only (A, AT, Dr, Dc)
-    std::vector<int4> blkA, blkT;
+    Scaled S;    // matrix part only: the unscaled A and AT on the host until they are uploaded, then Dr and Dc
+    std::map<int, std::pair<std::vector<int4>, std::vector<int4>>> blk;  // pack width -> row blocks of A, A^T
     int pbaseA = 0, pbaseT = 0;
-    int64_t nnzbase = 0;
+    int64_t nnzbase = 0, nnz = 0;
+    int dr_off = 0, dc_off = 0;  // offsets of this matrix's Dr / Dc in the device scaling scratch
 };
 
-uint64_t fnv(const void* p, size_t n, uint64_t h) {
+uint64_t fnv(const void* p, size_t n, uint64_t h) {  // FNV-1a over 8-byte words, then the tail bytes
     const unsigned char* b = static_cast<const unsigned char*>(p);
-    for (size_t i = 0; i < n; ++i) h = (h ^ b[i]) * 1099511628211ull;
+    size_t i = 0;
+    for (; i + 8 <= n; i += 8) {
+        uint64_t w;
+        std::memcpy(&w, b + i, 8);
+        h = (h ^ w) * 1099511628211ull;
+    }
+    for (; i < n; ++i) h = (h ^ b[i]) * 1099511628211ull;
     return h;
 }
 
@@ -340,18 +632,31 @@ struct BatchBase {
 template <class T>
 struct Batch final : BatchBase {
     int ninst = 0, M = 0, N = 0, nA = 0, nT = 0, freq = 64;
+    int nA1 = 0, nT1 = 0, nAp = 0, nTp = 0;  // iteration CTAs: width-1 packs (k_rowblock_batch), wider packs
+    int nAg = 0, nTg = 0;                     // iteration CTAs of instance groups (k_group_spmv)
+    int *A_grp = nullptr, *T_grp = nullptr;
+    int4 *A_git = nullptr, *T_git = nullptr, *gextA = nullptr, *gextT = nullptr;
     Options opt;
     std::vector<const taral_model*> models;
     std::vector<int> mat_of;                 // instance -> distinct matrix
     std::vector<std::unique_ptr<Shared>> mats;
     std::vector<Scaled> vecs;                // per instance: vector part
-    std::vector<int> row_off, col_off;
+    struct Pack {  // up to 8 instances sharing one matrix; vector entry (slot t, row r) at base + r * W + t
+        int mat = 0, W = 1, rbase = 0, cbase = 0;
+        int inst[8] = {-1, -1, -1, -1, -1, -1, -1, -1};
+    };
+    std::vector<Pack> packs;
+    std::vector<int2> where;  // instance -> {pack, slot}
+    int xidx(int i, int j) const { const Pack& q = packs[where[i].x]; return q.cbase + j * q.W + where[i].y; }
+    int zidx(int i, int r) const { const Pack& q = packs[where[i].x]; return q.rbase + r * q.W + where[i].y; }
     // device
     int *Aptr = nullptr, *Aidx = nullptr, *Tptr = nullptr, *Tidx = nullptr;
     T *Aval = nullptr, *Tval = nullptr;
     int4 *A_it = nullptr, *Ae_it = nullptr, *T_it = nullptr, *Te_it = nullptr;
+    int4 *A1_it = nullptr, *Ae1_it = nullptr, *T1_it = nullptr, *Te1_it = nullptr;
     int4 *A_ev = nullptr, *Ae_ev = nullptr, *T_ev = nullptr, *Te_ev = nullptr;
-    int *rr = nullptr, *cr = nullptr;
+    int *rr = nullptr, *cr = nullptr, *slot_inst = nullptr;
+    int2* d_where = nullptr;
     T *c = nullptr, *l = nullptr, *u = nullptr, *Dc = nullptr, *rl = nullptr, *ru = nullptr, *Dr = nullptr;
     double* par = nullptr;  // per instance {tau, sigma}
     T *x = nullptr, *ATz = nullptr, *xlast = nullptr, *z = nullptr, *Ax = nullptr, *zlast = nullptr;
@@ -395,10 +700,17 @@ struct Batch final : BatchBase {
         BK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
         // 1. distinct matrices (same sizes and identical col_ptr / row_idx / val)
         std::map<std::pair<uint64_t, std::pair<int, int>>, int> seen;
+        std::map<std::tuple<const void*, const void*, const void*, int, int>, int> same_arrays;
         mat_of.resize(count);
         for (int i = 0; i < count; ++i) {
             const taral_model& m = md[i];
             int64_t nz = m.col_ptr[m.n];
+            const auto akey = std::make_tuple((const void*)m.col_ptr, (const void*)m.row_idx, (const void*)m.val, m.m, m.n);
+            auto sa = same_arrays.find(akey);
+            if (sa != same_arrays.end()) {  // the very arrays of an earlier instance: the same matrix
+                mat_of[i] = sa->second;
+                continue;
+            }
             uint64_t h = 1469598103934665603ull;
             h = fnv(m.col_ptr, size_t(m.n + 1) * sizeof(int64_t), h);
             h = fnv(m.row_idx, size_t(nz) * sizeof(int32_t), h);
@@ -422,9 +734,10 @@ struct Batch final : BatchBase {
                 if (it == seen.end()) seen[key] = id;
                 mat_of[i] = id;
             }
+            same_arrays[akey] = mat_of[i];
         }
         distinct = int(mats.size());
-        // 2. scale: matrices (threads), then per-instance vectors
+        // 2. unscaled matrices (host transposes, threads over matrices); scaled on the device in step 3
         unsigned hw = std::max(1u, std::thread::hardware_concurrency());
         auto par_for = [&](int n, auto&& fn) {
             std::vector<std::thread> th;
@@ -438,81 +751,200 @@ struct Batch final : BatchBase {
         };
         par_for(distinct, [&](int k) {
             Shared& sh = *mats[k];
-            scale_matrix(md[first_inst[k]], sh.S);
-            sh.blkA = build_row_blocks(sh.S.A.ptr.data(), sh.S.A.rows);
-            sh.blkT = build_row_blocks(sh.S.AT.ptr.data(), sh.S.AT.rows);
+            const taral_model& mk = md[first_inst[k]];
+            model_matrices(mk, sh.S.A, sh.S.AT, 1);
+            sh.S.m = mk.m, sh.S.n = mk.n, sh.nnz = int64_t(sh.S.A.idx.size());
         });
+        // 3. concatenated matrices (int32 offsets), uploaded unscaled and scaled on the device (scaling.cuh:
+        //    bit-identical to scale_matrix), values narrowed to T in place
+        std::vector<int> hAptr, hTptr;
+        int64_t nzb = 0;
+        int drn = 0, dcn = 0;
+        for (auto& shp : mats) {
+            Shared& sh = *shp;
+            sh.pbaseA = int(hAptr.size()), sh.pbaseT = int(hTptr.size()), sh.nnzbase = nzb;
+            sh.dr_off = drn, sh.dc_off = dcn;
+            drn += sh.S.m, dcn += sh.S.n;
+            for (int64_t v : sh.S.A.ptr) hAptr.push_back(int(v + nzb));
+            for (int64_t v : sh.S.AT.ptr) hTptr.push_back(int(v + nzb));
+            nzb += sh.nnz;
+            if (nzb > INT32_MAX - 64) throw BatchError{"more than 2^31 distinct nonzeros in a batch"};
+        }
+        nnz_stored = nzb;
+        Aptr = put(hAptr), Tptr = put(hTptr);
+        Aidx = alloc<int>(size_t(nzb)), Tidx = alloc<int>(size_t(nzb));
+        Aval = alloc<T>(size_t(nzb)), Tval = alloc<T>(size_t(nzb));
+        {
+            struct Scratch {
+                std::vector<void*> p;
+                ~Scratch() { for (void* q : p) cudaFree(q); }
+            } tmp;
+            auto scratch = [&](size_t k) {
+                void* q = nullptr;
+                BK(cudaMalloc(&q, std::max<size_t>(k, 1) * sizeof(double)));
+                tmp.p.push_back(q);
+                return static_cast<double*>(q);
+            };
+            double *va, *vt;
+            if (sizeof(T) == sizeof(double)) va = reinterpret_cast<double*>(Aval), vt = reinterpret_cast<double*>(Tval);
+            else va = scratch(size_t(nzb)), vt = scratch(size_t(nzb));
+            double *dr = scratch(size_t(drn)), *dc = scratch(size_t(dcn)), *rs = scratch(size_t(drn)),
+                   *cs = scratch(size_t(dcn));
+            for (auto& shp : mats) {
+                Shared& sh = *shp;
+                const size_t nz = size_t(sh.nnz), b = size_t(sh.nnzbase);
+                if (nz) {
+                    BK(cudaMemcpyAsync(Aidx + b, sh.S.A.idx.data(), nz * sizeof(int), cudaMemcpyHostToDevice, s));
+                    BK(cudaMemcpyAsync(Tidx + b, sh.S.AT.idx.data(), nz * sizeof(int), cudaMemcpyHostToDevice, s));
+                    BK(cudaMemcpyAsync(va + b, sh.S.A.val.data(), nz * sizeof(double), cudaMemcpyHostToDevice, s));
+                    BK(cudaMemcpyAsync(vt + b, sh.S.AT.val.data(), nz * sizeof(double), cudaMemcpyHostToDevice, s));
+                }
+                scale_on_device(sh.S.m, sh.S.n, Aptr + sh.pbaseA, Aidx, va, Tptr + sh.pbaseT, Tidx, vt,
+                                dr + sh.dr_off, dc + sh.dc_off, rs + sh.dr_off, cs + sh.dc_off, s);
+            }
+            if (sizeof(T) != sizeof(double) && nzb) {
+                const int g = int(std::min<int64_t>((nzb + 255) / 256, 148 * 16));
+                k_narrow<T><<<g, 256, 0, s>>>(nzb, va, Aval);
+                k_narrow<T><<<g, 256, 0, s>>>(nzb, vt, Tval);
+            }
+            std::vector<double> hdr(static_cast<size_t>(drn)), hdc(static_cast<size_t>(dcn));
+            if (drn) BK(cudaMemcpyAsync(hdr.data(), dr, size_t(drn) * sizeof(double), cudaMemcpyDeviceToHost, s));
+            if (dcn) BK(cudaMemcpyAsync(hdc.data(), dc, size_t(dcn) * sizeof(double), cudaMemcpyDeviceToHost, s));
+            BK(cudaStreamSynchronize(s));
+            BK(cudaGetLastError());
+            for (auto& shp : mats) {
+                Shared& sh = *shp;
+                sh.S.Dr.assign(hdr.begin() + sh.dr_off, hdr.begin() + sh.dr_off + sh.S.m);
+                sh.S.Dc.assign(hdc.begin() + sh.dc_off, hdc.begin() + sh.dc_off + sh.S.n);
+                for (Csr* h : {&sh.S.A, &sh.S.AT}) {  // keep the row pointers (block lists), drop the entries
+                    h->idx.clear(), h->idx.shrink_to_fit();
+                    h->val.clear(), h->val.shrink_to_fit();
+                }
+            }
+        }
         vecs.resize(count);
         par_for(count, [&](int i) {
             const Shared& sh = *mats[mat_of[i]];
             scale_vectors(md[i], md[i].maximize ? -1.0 : 1.0, sh.S.Dr, sh.S.Dc, vecs[i]);
         });
-        // 3. concatenated matrices (int32 offsets)
-        std::vector<int> hAptr, hTptr, hAidx, hTidx;
-        std::vector<T> hAval, hTval;
-        int64_t nzb = 0;
-        for (auto& shp : mats) {
-            Shared& sh = *shp;
-            sh.pbaseA = int(hAptr.size()), sh.pbaseT = int(hTptr.size()), sh.nnzbase = nzb;
-            for (int64_t v : sh.S.A.ptr) hAptr.push_back(int(v + nzb));
-            for (int64_t v : sh.S.AT.ptr) hTptr.push_back(int(v + nzb));
-            hAidx.insert(hAidx.end(), sh.S.A.idx.begin(), sh.S.A.idx.end());
-            hTidx.insert(hTidx.end(), sh.S.AT.idx.begin(), sh.S.AT.idx.end());
-            for (double v : sh.S.A.val) hAval.push_back(T(v));
-            for (double v : sh.S.AT.val) hTval.push_back(T(v));
-            nzb += int64_t(sh.S.A.val.size());
-            if (nzb > INT32_MAX - 64) throw BatchError{"more than 2^31 distinct nonzeros in a batch"};
+        // 4. packs (instances of one matrix, 8 slots, the remainder in the smallest power of two) and block lists
+        std::vector<std::vector<int>> users(distinct);
+        for (int i = 0; i < count; ++i) users[mat_of[i]].push_back(i);
+        std::vector<std::vector<int>> packs_of(distinct);
+        int pack_cap = 1;  // widest pack; TARAL_BATCH_PACK = 1, 2, 4 or 8 overrides
+        if (const char* e = std::getenv("TARAL_BATCH_PACK")) {
+            const int v = std::atoi(e);
+            pack_cap = v >= 8 ? 8 : v >= 4 ? 4 : v >= 2 ? 2 : 1;
         }
-        nnz_stored = nzb;
-        // 4. instance offsets and block lists
-        row_off.assign(count + 1, 0), col_off.assign(count + 1, 0);
-        for (int i = 0; i < count; ++i) row_off[i + 1] = row_off[i] + md[i].m, col_off[i + 1] = col_off[i] + md[i].n;
-        M = row_off[count], N = col_off[count];
-        if (int64_t(M) + N > INT32_MAX - 1024) throw BatchError{"batch too large for int32 indexing"};
+        where.assign(count, make_int2(0, 0));
+        int64_t Mt = 0, Nt = 0;
+        for (int k = 0; k < distinct; ++k) {
+            const Shared& sh = *mats[k];
+            for (size_t u0 = 0; u0 < users[k].size();) {
+                const int rem = int(users[k].size() - u0);
+                Pack q;  // width: the smallest power of two holding the remaining instances, at most pack_cap
+                q.mat = k, q.W = std::min(pack_cap, rem > 4 ? 8 : rem > 2 ? 4 : rem);
+                const int used = std::min(rem, q.W);
+                q.rbase = int(Mt), q.cbase = int(Nt);
+                Mt += int64_t(sh.S.m) * q.W, Nt += int64_t(sh.S.n) * q.W;
+                for (int t = 0; t < used; ++t) q.inst[t] = users[k][u0 + t], where[users[k][u0 + t]] = make_int2(int(packs.size()), t);
+                packs_of[k].push_back(int(packs.size()));
+                packs.push_back(q);
+                u0 += size_t(used);
+            }
+            Shared& shw = *mats[k];
+            for (int p : packs_of[k]) {
+                const int W = packs[p].W;
+                if (!shw.blk.count(W))
+                    shw.blk[W] = {build_row_blocks(shw.S.A.ptr.data(), shw.S.m, pack_tile(W), kRowsMax / W),
+                                  build_row_blocks(shw.S.AT.ptr.data(), shw.S.n, pack_tile(W), kRowsMax / W)};
+            }
+        }
+        if (Mt + Nt > INT32_MAX - 1024) throw BatchError{"batch too large for int32 indexing"};
+        M = int(Mt), N = int(Nt);
         std::vector<int4> a_it, ae_it, t_it, te_it, a_ev, ae_ev, t_ev, te_ev;
-        std::vector<int> hrr{0}, hcr{0};
-        auto shiftA = [&](int i) {
-            const Shared& sh = *mats[mat_of[i]];
-            return make_int4(i, row_off[i] - sh.pbaseA, col_off[i], 0);
-        };
-        auto shiftT = [&](int i) {
-            const Shared& sh = *mats[mat_of[i]];
-            return make_int4(i, col_off[i] - sh.pbaseT, row_off[i], 0);
-        };
+        std::vector<int> hrr{0}, hcr{0}, hslot;
         auto rebase = [](int4 b, int pbase, int64_t nzbase) {
             return make_int4(b.x + pbase, b.y, int(b.z + nzbase), int(b.w + nzbase));
         };
-        for (int i = 0; i < count; ++i) {  // evaluation order: instance-major
-            const Shared& sh = *mats[mat_of[i]];
-            for (const int4& b : sh.blkA) a_ev.push_back(rebase(b, sh.pbaseA, sh.nnzbase)), ae_ev.push_back(shiftA(i));
-            for (const int4& b : sh.blkT) t_ev.push_back(rebase(b, sh.pbaseT, sh.nnzbase)), te_ev.push_back(shiftT(i));
+        auto extA = [&](int p, const int4& b) { const Pack& q = packs[p]; return make_int4(p, q.rbase + b.x * q.W, q.cbase, q.W); };
+        auto extT = [&](int p, const int4& b) { const Pack& q = packs[p]; return make_int4(p, q.cbase + b.x * q.W, q.rbase, q.W); };
+        for (int p = 0; p < int(packs.size()); ++p) {  // evaluation order: pack-major
+            const Shared& sh = *mats[packs[p].mat];
+            const auto& bl = sh.blk.at(packs[p].W);
+            for (const int4& b : bl.first) a_ev.push_back(rebase(b, sh.pbaseA, sh.nnzbase)), ae_ev.push_back(extA(p, b));
+            for (const int4& b : bl.second) t_ev.push_back(rebase(b, sh.pbaseT, sh.nnzbase)), te_ev.push_back(extT(p, b));
             hrr.push_back(int(a_ev.size())), hcr.push_back(int(t_ev.size()));
+            for (int t = 0; t < 8; ++t) hslot.push_back(packs[p].inst[t]);
         }
-        std::vector<std::vector<int>> users(distinct);
-        for (int i = 0; i < count; ++i) users[mat_of[i]].push_back(i);
-        for (int k = 0; k < distinct; ++k) {  // iteration order: matrix-major, instances interleaved per tile
+        // iteration order: matrix-major, the packs of one width interleaved per block. Width-1 packs (one instance)
+        // run on the single-instance skeleton k_rowblock_batch, whose block extension is {instance, row shift,
+        // gather offset, 0}; wider packs on k_pack_spmv.
+        std::vector<int4> a1_it, ae1_it, t1_it, te1_it;
+        bool grouping = false;  // TARAL_BATCH_GROUP=1: one CTA per (block, group of instances) instead of per instance
+        if (const char* e = std::getenv("TARAL_BATCH_GROUP")) grouping = std::atoi(e) != 0;
+        std::vector<int4> ga_it, gt_it, hgA, hgT;
+        std::vector<int> ga_grp, gt_grp;
+        for (int k = 0; k < distinct && grouping; ++k) {
             const Shared& sh = *mats[k];
-            for (const int4& b : sh.blkA)
-                for (int i : users[k]) a_it.push_back(rebase(b, sh.pbaseA, sh.nnzbase)), ae_it.push_back(shiftA(i));
-            for (const int4& b : sh.blkT)
-                for (int i : users[k]) t_it.push_back(rebase(b, sh.pbaseT, sh.nnzbase)), te_it.push_back(shiftT(i));
+            std::vector<int> ones;
+            for (int p : packs_of[k])
+                if (packs[p].W == 1) ones.push_back(p);
+            if (ones.empty()) continue;
+            const auto& bl = sh.blk.at(1);
+            for (size_t g0 = 0; g0 < ones.size(); g0 += kGroup) {
+                const int gid = int(hgA.size() / kGroup);
+                for (int t = 0; t < kGroup; ++t) {
+                    const bool in = g0 + t < ones.size();
+                    const Pack& q = packs[in ? ones[g0 + t] : ones[0]];
+                    hgA.push_back(in ? make_int4(q.inst[0], q.rbase - sh.pbaseA, q.cbase, 0) : make_int4(-1, 0, 0, 0));
+                    hgT.push_back(in ? make_int4(q.inst[0], q.cbase - sh.pbaseT, q.rbase, 0) : make_int4(-1, 0, 0, 0));
+                }
+                for (const int4& b : bl.first) ga_it.push_back(rebase(b, sh.pbaseA, sh.nnzbase)), ga_grp.push_back(gid);
+                for (const int4& b : bl.second) gt_it.push_back(rebase(b, sh.pbaseT, sh.nnzbase)), gt_grp.push_back(gid);
+            }
         }
-        nA = int(a_it.size()), nT = int(t_it.size());
+        nAg = int(ga_it.size()), nTg = int(gt_it.size());
+        A_git = put(ga_it), T_git = put(gt_it), A_grp = put(ga_grp), T_grp = put(gt_grp), gextA = put(hgA), gextT = put(hgT);
+        for (int k = 0; k < distinct; ++k) {
+            const Shared& sh = *mats[k];
+            for (const auto& wb : sh.blk) {
+                const bool one = wb.first == 1;
+                if (one && grouping) continue;  // served by the groups
+                for (const int4& b : wb.second.first)
+                    for (int p : packs_of[k]) {
+                        if (packs[p].W != wb.first) continue;
+                        const int4 rb = rebase(b, sh.pbaseA, sh.nnzbase);
+                        if (one) a1_it.push_back(rb), ae1_it.push_back(make_int4(packs[p].inst[0], packs[p].rbase - sh.pbaseA, packs[p].cbase, 0));
+                        else a_it.push_back(rb), ae_it.push_back(extA(p, b));
+                    }
+                for (const int4& b : wb.second.second)
+                    for (int p : packs_of[k]) {
+                        if (packs[p].W != wb.first) continue;
+                        const int4 rb = rebase(b, sh.pbaseT, sh.nnzbase);
+                        if (one) t1_it.push_back(rb), te1_it.push_back(make_int4(packs[p].inst[0], packs[p].cbase - sh.pbaseT, packs[p].rbase, 0));
+                        else t_it.push_back(rb), te_it.push_back(extT(p, b));
+                    }
+            }
+        }
+        nA = int(a_ev.size()), nT = int(t_ev.size());
+        nA1 = int(a1_it.size()), nT1 = int(t1_it.size()), nAp = int(a_it.size()), nTp = int(t_it.size());
+        A1_it = put(a1_it), Ae1_it = put(ae1_it), T1_it = put(t1_it), Te1_it = put(te1_it);
+        slot_inst = put(hslot), d_where = put(where);
         // 5. upload
-        Aptr = put(hAptr), Tptr = put(hTptr), Aidx = put(hAidx), Tidx = put(hTidx), Aval = put(hAval), Tval = put(hTval);
         A_it = put(a_it), Ae_it = put(ae_it), T_it = put(t_it), Te_it = put(te_it);
         A_ev = put(a_ev), Ae_ev = put(ae_ev), T_ev = put(t_ev), Te_ev = put(te_ev);
         rr = put(hrr), cr = put(hcr);
-        std::vector<T> hc(N), hl(N), hu(N), hDc(N), hrl(M), hru(M), hDr(M);
+        std::vector<T> hc(N, T(0)), hl(N, T(0)), hu(N, T(0)), hDc(N, T(1)), hrl(M, T(0)), hru(M, T(0)), hDr(M, T(1));
         for (int i = 0; i < count; ++i) {
             const Scaled& v = vecs[i];
             const Shared& sh = *mats[mat_of[i]];
             for (int j = 0; j < md[i].n; ++j) {
-                int g = col_off[i] + j;
+                const int g = xidx(i, j);
                 hc[g] = T(v.c[j]), hl[g] = T(v.l[j]), hu[g] = T(v.u[j]), hDc[g] = T(sh.S.Dc[j]);
             }
             for (int r = 0; r < md[i].m; ++r) {
-                int g = row_off[i] + r;
+                const int g = zidx(i, r);
                 hrl[g] = T(v.rl[r]), hru[g] = T(v.ru[r]), hDr[g] = T(sh.S.Dr[r]);
             }
         }
@@ -521,7 +953,7 @@ struct Batch final : BatchBase {
         pv = alloc<T>(N), pu = alloc<T>(N), pw = alloc<T>(M);
         xs = alloc<double>(N), zs = alloc<double>(M), tmpM = alloc<double>(M), tmpN = alloc<double>(N);
         dout = alloc<double>(size_t(std::max(M, N)));
-        partA = alloc<double>(size_t(std::max(nA, 1)) * 5), partT = alloc<double>(size_t(std::max(nT, 1)) * 5);
+        partA = alloc<double>(size_t(std::max(nA, 1)) * 40), partT = alloc<double>(size_t(std::max(nT, 1)) * 40);
         kkt = alloc<double>(size_t(count) * 20), fbuf = alloc<double>(count), est = alloc<double>(count);
         pscale = alloc<double>(count), st = alloc<InstState>(count), par = alloc<double>(2 * size_t(count));
         running = alloc<int>(count), rflag = alloc<int>(count), pactive = alloc<int>(count), this->count = alloc<int>(1);
@@ -531,7 +963,7 @@ struct Batch final : BatchBase {
         BK(cudaMemGetInfo(&free1, &total));
         mem_used = free0 - free1;
         nnz_total = 0;
-        for (int i = 0; i < count; ++i) nnz_total += int64_t(mats[mat_of[i]]->S.A.val.size());
+        for (int i = 0; i < count; ++i) nnz_total += mats[mat_of[i]]->nnz;
         models.clear();
         for (int i = 0; i < count; ++i) models.push_back(md + i);
     }
@@ -540,11 +972,15 @@ struct Batch final : BatchBase {
     // ------------------------------------------------------------------ launches
     template <class X, class E>
     void spmv_A(const X* xin, const E& e, const int* act) {
-        if (nA) k_rowblock_batch<T, X, E, true><<<nA, kThreads, 0, s>>>(Aptr, Aidx, Aval, xin, A_it, Ae_it, act, e), ++launches;
+        if (nAg) k_group_spmv<T, X, E><<<nAg, kThreads, 0, s>>>(Aptr, Aidx, Aval, xin, A_git, A_grp, gextA, act, e), ++launches;
+        if (nA1) k_rowblock_batch<T, X, E, true><<<nA1, kThreads, 0, s>>>(Aptr, Aidx, Aval, xin, A1_it, Ae1_it, act, e), ++launches;
+        if (nAp) k_pack_spmv<T, X, E><<<nAp, kThreads, 0, s>>>(Aptr, Aidx, Aval, xin, A_it, Ae_it, slot_inst, act, e), ++launches;
     }
     template <class X, class E>
     void spmv_T(const X* xin, const E& e, const int* act) {
-        if (nT) k_rowblock_batch<T, X, E, true><<<nT, kThreads, 0, s>>>(Tptr, Tidx, Tval, xin, T_it, Te_it, act, e), ++launches;
+        if (nTg) k_group_spmv<T, X, E><<<nTg, kThreads, 0, s>>>(Tptr, Tidx, Tval, xin, T_git, T_grp, gextT, act, e), ++launches;
+        if (nT1) k_rowblock_batch<T, X, E, true><<<nT1, kThreads, 0, s>>>(Tptr, Tidx, Tval, xin, T1_it, Te1_it, act, e), ++launches;
+        if (nTp) k_pack_spmv<T, X, E><<<nTp, kThreads, 0, s>>>(Tptr, Tidx, Tval, xin, T_it, Te_it, slot_inst, act, e), ++launches;
     }
     void products(const int* act) {
         spmv_A(x, EpiStore<T>{Ax}, act);
@@ -553,19 +989,19 @@ struct Batch final : BatchBase {
     void eval_into(double* dst, bool avg, const int* act) {
         const double* fi = avg ? fbuf : nullptr;
         if (!avg) {
-            if (nA) k_eval_blocks<T, T, true><<<nA, kThreads, 0, s>>>(A_ev, Ae_ev, act, fi, Ax, z, rl, ru, nullptr, Dr, zlast, partA);
-            if (nT) k_eval_blocks<T, T, false><<<nT, kThreads, 0, s>>>(T_ev, Te_ev, act, fi, x, ATz, l, u, c, Dc, xlast, partT);
+            if (nA) k_pack_eval<T, T, true><<<nA, kThreads, 0, s>>>(A_ev, Ae_ev, slot_inst, act, fi, Ax, z, rl, ru, nullptr, Dr, zlast, partA);
+            if (nT) k_pack_eval<T, T, false><<<nT, kThreads, 0, s>>>(T_ev, Te_ev, slot_inst, act, fi, x, ATz, l, u, c, Dc, xlast, partT);
         } else {
             spmv_A(xs, EpiStore<double>{tmpM}, act);
             spmv_T(zs, EpiStore<double>{tmpN}, act);
-            if (nA) k_eval_blocks<T, double, true><<<nA, kThreads, 0, s>>>(A_ev, Ae_ev, act, fi, tmpM, zs, rl, ru, nullptr, Dr, zlast, partA);
-            if (nT) k_eval_blocks<T, double, false><<<nT, kThreads, 0, s>>>(T_ev, Te_ev, act, fi, xs, tmpN, l, u, c, Dc, xlast, partT);
+            if (nA) k_pack_eval<T, double, true><<<nA, kThreads, 0, s>>>(A_ev, Ae_ev, slot_inst, act, fi, tmpM, zs, rl, ru, nullptr, Dr, zlast, partA);
+            if (nT) k_pack_eval<T, double, false><<<nT, kThreads, 0, s>>>(T_ev, Te_ev, slot_inst, act, fi, xs, tmpN, l, u, c, Dc, xlast, partT);
         }
-        k_eval_finish<<<(ninst + 7) / 8, 256, 0, s>>>(ninst, rr, cr, partA, partT, act, dst);
+        k_eval_finish<<<(ninst + 7) / 8, 256, 0, s>>>(ninst, d_where, rr, cr, partA, partT, act, dst);
         launches += 3;
     }
     void block(int steps) {
-        if (nT) k_xupd_blocks<T><<<nT, kThreads, 0, s>>>(T_ev, Te_ev, running, x, ATz, c, l, u, par, xs), ++launches;
+        if (nT) k_pack_xupd<T><<<nT, kThreads, 0, s>>>(T_ev, Te_ev, slot_inst, running, x, ATz, c, l, u, par, xs), ++launches;
         for (int k = 0; k < steps; ++k) {
             spmv_A(x, EpiRow<T>{Ax, z, zs, rl, ru, par}, running);
             spmv_T(z, EpiCol<T>{ATz, x, xs, c, l, u, par, k + 1 < steps ? 1 : 0}, running);
@@ -577,8 +1013,8 @@ struct Batch final : BatchBase {
         eval_into(kkt + 10 * size_t(ninst), true, running);
         k_decide<T><<<g, 256, 0, s>>>(ninst, st, kkt, kkt + 10 * size_t(ninst), par, running, rflag, opt.tol,
                                       opt.row_rel, (long long)opt.max_iter, d_deadline);
-        if (nT) k_restart_blocks<T><<<nT, kThreads, 0, s>>>(T_ev, Te_ev, rflag, st, x, xs, xlast);
-        if (nA) k_restart_blocks<T><<<nA, kThreads, 0, s>>>(A_ev, Ae_ev, rflag, st, z, zs, zlast);
+        if (nT) k_pack_restart<T><<<nT, kThreads, 0, s>>>(T_ev, Te_ev, slot_inst, rflag, st, x, xs, xlast);
+        if (nA) k_pack_restart<T><<<nA, kThreads, 0, s>>>(A_ev, Ae_ev, slot_inst, rflag, st, z, zs, zlast);
         products(rflag);
         k_count<<<1, 256, 0, s>>>(ninst, running, count);
         launches += 7;
@@ -596,9 +1032,10 @@ struct Batch final : BatchBase {
         for (int i = 0; i < ninst; ++i) {
             int n = models[i]->n;
             double nn = 0;
-            for (int j = 0; j < n; ++j) h[col_off[i] + j] = 0.5 + double((uint32_t(j) * 2654435761u) % 1000u) / 1000.0;
-            for (int j = 0; j < n; ++j) nn += h[col_off[i] + j] * h[col_off[i] + j];
-            for (int j = 0; j < n; ++j) h[col_off[i] + j] = h[col_off[i] + j] / std::sqrt(nn);
+            std::vector<double> v0(static_cast<size_t>(n));
+            for (int j = 0; j < n; ++j) v0[j] = 0.5 + double((uint32_t(j) * 2654435761u) % 1000u) / 1000.0;
+            for (int j = 0; j < n; ++j) nn += v0[j] * v0[j];
+            for (int j = 0; j < n; ++j) h[xidx(i, j)] = v0[j] / std::sqrt(nn);
         }
         BK(cudaMemcpyAsync(dout, h.data(), size_t(N) * sizeof(double), cudaMemcpyHostToDevice, s));
         k_cast<T><<<std::max(1, std::min((N + 255) / 256, 1184)), 256, 0, s>>>(N, dout, pv);
@@ -612,9 +1049,9 @@ struct Batch final : BatchBase {
             for (; it < end; ++it) {
                 spmv_A(a, EpiStore<T>{pw}, pactive);
                 spmv_T(pw, EpiStore<T>{b}, pactive);
-                if (nT) k_pow_part<T><<<nT, kThreads, 0, s>>>(T_ev, Te_ev, pactive, b, partT);
-                k_pow_update<<<g, 256, 0, s>>>(ninst, cr, partT, est, pscale, pactive, it);
-                if (nT) k_pow_scale<T><<<nT, kThreads, 0, s>>>(T_ev, Te_ev, pactive, pscale, b);
+                if (nT) k_pack_pow_part<T><<<nT, kThreads, 0, s>>>(T_ev, Te_ev, slot_inst, pactive, b, partT);
+                k_pow_update<<<g, 256, 0, s>>>(ninst, d_where, cr, partT, est, pscale, pactive, it);
+                if (nT) k_pack_pow_scale<T><<<nT, kThreads, 0, s>>>(T_ev, Te_ev, slot_inst, pactive, pscale, b);
                 launches += 3;
                 std::swap(a, b);
             }
@@ -670,9 +1107,9 @@ struct Batch final : BatchBase {
             for (int i = 0; i < ninst; ++i) {
                 const Shared& sh = *mats[mat_of[i]];
                 if (x0 && x0[i])
-                    for (int j = 0; j < models[i]->n; ++j) hx[col_off[i] + j] = T(x0[i][j] / sh.S.Dc[j]);
+                    for (int j = 0; j < models[i]->n; ++j) hx[xidx(i, j)] = T(x0[i][j] / sh.S.Dc[j]);
                 if (y0 && y0[i])
-                    for (int r = 0; r < models[i]->m; ++r) hz[row_off[i] + r] = T(y0[i][r] / sh.S.Dr[r]);
+                    for (int r = 0; r < models[i]->m; ++r) hz[zidx(i, r)] = T(y0[i][r] / sh.S.Dr[r]);
             }
             BK(cudaMemcpyAsync(x, hx.data(), N * sizeof(T), cudaMemcpyHostToDevice, s));
             BK(cudaMemcpyAsync(xlast, hx.data(), N * sizeof(T), cudaMemcpyHostToDevice, s));
@@ -719,9 +1156,9 @@ struct Batch final : BatchBase {
         std::vector<InstState> fin(ninst);
         BK(cudaMemcpyAsync(fin.data(), st, ninst * sizeof(InstState), cudaMemcpyDeviceToHost, s));
         std::vector<double> hx(N), hz(M);
-        if (nT) k_out_blocks<T><<<nT, kThreads, 0, s>>>(T_ev, Te_ev, st, x, xs, dout);
+        if (nT) k_pack_out<T><<<nT, kThreads, 0, s>>>(T_ev, Te_ev, slot_inst, st, x, xs, dout);
         BK(cudaMemcpyAsync(hx.data(), dout, N * sizeof(double), cudaMemcpyDeviceToHost, s));
-        if (nA) k_out_blocks<T><<<nA, kThreads, 0, s>>>(A_ev, Ae_ev, st, z, zs, dout);
+        if (nA) k_pack_out<T><<<nA, kThreads, 0, s>>>(A_ev, Ae_ev, slot_inst, st, z, zs, dout);
         BK(cudaMemcpyAsync(hz.data(), dout, M * sizeof(double), cudaMemcpyDeviceToHost, s));
         BK(cudaEventRecord(e1, s));
         BK(cudaStreamSynchronize(s));
@@ -736,8 +1173,9 @@ struct Batch final : BatchBase {
             Outcome r;
             r.status = q.status, r.iterations = q.it, r.restarts = q.restarts, r.from_average = q.avg_final != 0;
             r.rel_primal = q.best_p, r.rel_dual = q.best_d, r.rel_gap = q.best_g, r.norm_a = q.norm, r.omega = q.w;
-            r.x.assign(hx.begin() + col_off[i], hx.begin() + col_off[i + 1]);
-            r.z.assign(hz.begin() + row_off[i], hz.begin() + row_off[i + 1]);
+            r.x.resize(size_t(models[i]->n)), r.z.resize(size_t(models[i]->m));
+            for (int j = 0; j < models[i]->n; ++j) r.x[j] = hx[xidx(i, j)];
+            for (int q = 0; q < models[i]->m; ++q) r.z[q] = hz[zidx(i, q)];
             Scaled P;  // finish_point needs Dr, Dc and sizes
             P.m = models[i]->m, P.n = models[i]->n, P.Dr = sh.S.Dr, P.Dc = sh.S.Dc;
             Finished f = finish_point(*models[i], P, r);
@@ -747,7 +1185,7 @@ struct Batch final : BatchBase {
             o.rel_primal = r.rel_primal, o.rel_dual = r.rel_dual, o.rel_gap = r.rel_gap, o.norm_a = r.norm_a;
             o.primal_weight = r.omega, o.objective = f.objective, o.max_row_violation = f.max_row_violation;
             o.max_bound_violation = f.max_bound_violation, o.solve_s = solve_s, o.power_iter_s = power_s;
-            o.device_mem_bytes = mem_used, o.kernel_launches = launches, o.nnz = int64_t(sh.S.A.val.size());
+            o.device_mem_bytes = mem_used, o.kernel_launches = launches, o.nnz = sh.nnz;
             o.device_s = ms * 1e-3;
             if (xo && xo[i]) std::memcpy(xo[i], f.x.data(), f.x.size() * sizeof(double));
             if (yo && yo[i]) std::memcpy(yo[i], f.y.data(), f.y.size() * sizeof(double));

@@ -31,20 +31,22 @@ namespace taral {
 // ---------------------------------------------------------------------------------------------- row blocks
 // Consecutive rows are packed into blocks of at most kTile nonzeros and kRowsMax rows; a longer row is a block of
 // its own (block_sums sums it with the whole CTA).
-std::vector<int4> build_row_blocks(const int64_t* ptr, int rows) {
+std::vector<int4> build_row_blocks(const int64_t* ptr, int rows) { return build_row_blocks(ptr, rows, kTile, kRowsMax); }
+
+std::vector<int4> build_row_blocks(const int64_t* ptr, int rows, int tile, int rows_max) {
     std::vector<int4> out;
     auto close = [&](int r0, int r1) { out.push_back(make_int4(r0, r1 - r0, int(ptr[r0]), int(ptr[r1]))); };
     int start = 0, cur_rows = 0;
     int64_t cur_nnz = 0;
     for (int r = 0; r < rows; ++r) {
         int64_t L = ptr[r + 1] - ptr[r];
-        if (L > kTile) {  // a long row is a block of its own
+        if (L > tile) {  // a long row is a block of its own
             if (cur_rows) close(start, r);
             close(r, r + 1);
             start = r + 1, cur_rows = 0, cur_nnz = 0;
             continue;
         }
-        if (cur_rows == kRowsMax || cur_nnz + L > kTile) close(start, r), start = r, cur_rows = 0, cur_nnz = 0;
+        if (cur_rows == rows_max || cur_nnz + L > tile) close(start, r), start = r, cur_rows = 0, cur_nnz = 0;
         ++cur_rows, cur_nnz += L;
     }
     if (cur_rows) close(start, rows);
@@ -173,8 +175,8 @@ struct Engine final : EngineBase {
     }
     // Set-up from the column-wise model with the scaling on the device (scaling.cuh): the host builds the unscaled
     // A and A^T (model_matrices, the reference's transposes), the device scales them in FP64 and narrows the values
-    // to T in place. Fills P's Dr, Dc, vectors and norms (scale_vectors on the host, O(m + n)) and nnz; P.A and
-    // P.AT stay empty. host_s: seconds of host work.
+    // to T in place. Fills P's Dr, Dc, vectors and norms (scale_vectors on the host, O(m + n)); P.A keeps the
+    // UNSCALED row-wise copy (for finish_point), P.AT stays empty. host_s: seconds of host work.
     void init_model(const taral_model& md, double sign, Scaled& P, int freq, unsigned flags, double* host_s) {
         auto t0 = Clock::now();
         Csr hA, hAT;
@@ -219,12 +221,12 @@ struct Engine final : EngineBase {
         CK(cudaGetLastError());
         }  // FP64 scratch released
         t0 = Clock::now();
-        hA = Csr(), hAT = Csr();
+        P.A = std::move(hA), P.AT = Csr();  // the unscaled row-wise copy serves the original-space check
+        P.a_original = true;
+        hAT = Csr();
         scale_vectors(md, sign, P.Dr, P.Dc, P);
         hs += since(t0);
         if (host_s) *host_s = hs;
-        P.A = Csr(), P.AT = Csr();
-        P.A.rows = m, P.AT.rows = n;
         finish_init(P.c.data(), P.l.data(), P.u.data(), P.rl.data(), P.ru.data(), P.Dr.data(), P.Dc.data());
         nnz = nz;
     }

@@ -42,6 +42,8 @@ void engine_init(EngineBase& e, int precision, const taral_csr& A, const taral_c
                  const double* l, const double* u, const double* rl, const double* ru, const double* Dr,
                  const double* Dc, int m, int n, int eval_freq, unsigned flags);
 std::vector<int4> build_row_blocks(const int64_t* ptr, int rows);
+// Blocks of at most `tile` nonzeros and `rows_max` rows (a longer row is a block of its own).
+std::vector<int4> build_row_blocks(const int64_t* ptr, int rows, int tile, int rows_max);
 // Set-up from the column-wise model with the scaling done on the device, bit-identical to build_scaled(): P gets
 // Dr, Dc, the scaled vectors and the norms (its matrices stay empty); host_s: seconds of host work.
 struct Scaled;

@@ -56,6 +56,7 @@ struct Scaled {
     Csr A, AT;
     std::vector<double> c, l, u, rl, ru, Dr, Dc;
     double bnorm = 0, cnorm = 0;  // original-space norms of the stopping test
+    bool a_original = false;      // A holds the UNSCALED row-wise matrix (device-side set-up), used by finish_point
 };
 Scaled build_scaled(const taral_model& md, double sign);  // gpu/pdhg.cu:80-133
 // The two halves of build_scaled: the matrix part (A_s, A_s^T, Dr, Dc: depends on A only) and the vector part

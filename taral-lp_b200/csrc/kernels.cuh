@@ -223,7 +223,15 @@ __device__ __forceinline__ void block_sums(const int* __restrict__ ptr, const in
         const int a = sm.rptr[tid], b = sm.rptr[tid + 1];
         if (b - a <= kShort) {
             double s = 0;
-            for (int k = a; k < b; ++k) s += double(sm.prod[pidx(k)]);
+            int k = a;
+            for (; k + 4 <= b; k += 4) {  // four loads in flight, then the adds in entry order
+                P t[4];
+#pragma unroll
+                for (int e = 0; e < 4; ++e) t[e] = sm.prod[pidx(k + e)];
+#pragma unroll
+                for (int e = 0; e < 4; ++e) s += double(t[e]);
+            }
+            for (; k < b; ++k) s += double(sm.prod[pidx(k)]);
             sm.rowsum[tid] = s;
         } else {
             sm.longrow[atomicAdd(&sm.nlong, 1)] = short(tid);

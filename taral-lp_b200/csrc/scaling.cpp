@@ -85,7 +85,20 @@ void model_matrices(const taral_model& md, Csr& A, Csr& AT, int threads) {
         }
         A = transpose_par(T.ptr.data(), T.idx.data(), T.val.data(), md.n, md.m, threads);
     }
-    AT = transpose_par(A.ptr.data(), A.idx.data(), A.val.data(), md.m, md.n, threads);
+    // A^T = transpose(A) has ascending row indices in every column; a model whose columns already list their rows
+    // in ascending order with no explicit zero is that matrix as it stands
+    bool sorted = !zeros;
+    for (int j = 0; j < md.n && sorted; ++j)
+        for (int64_t k = md.col_ptr[j] + 1; k < md.col_ptr[j + 1] && sorted; ++k) sorted = md.row_idx[k - 1] < md.row_idx[k];
+    if (sorted) {
+        AT.rows = md.n;
+        AT.ptr.assign(md.col_ptr, md.col_ptr + md.n + 1);
+        for (int64_t& v : AT.ptr) v -= k0;
+        AT.idx.assign(md.row_idx + k0, md.row_idx + k1);
+        AT.val.assign(md.val + k0, md.val + k1);
+    } else {
+        AT = transpose_par(A.ptr.data(), A.idx.data(), A.val.data(), md.m, md.n, threads);
+    }
 }
 
 void scale_matrix(const taral_model& md, Scaled& P) {
@@ -173,13 +186,39 @@ Finished finish_point(const taral_model& md, const Scaled& P, const Outcome& r) 
     for (int i = 0; i < P.m; ++i) f.y[i] = P.Dr[i] * r.z[i];
     long double obj = md.obj_const;
     for (int j = 0; j < P.n; ++j) obj += (long double)md.cost[j] * f.x[j];
-    std::vector<double> ax(size_t(P.m), 0.0);
     double bviol = 0, rviol = 0;
+    bool finite = true;
     for (int j = 0; j < P.n; ++j) {
-        for (int64_t k = md.col_ptr[j]; k < md.col_ptr[j + 1]; ++k) ax[md.row_idx[k]] += md.val[k] * f.x[j];
         bviol = std::max(bviol, std::max(md.col_lo[j] - f.x[j], f.x[j] - md.col_up[j]));
+        finite = finite && std::isfinite(f.x[j]);
     }
-    for (int i = 0; i < P.m; ++i) rviol = std::max(rviol, std::max(md.row_lo[i] - ax[i], ax[i] - md.row_up[i]));
+    if (finite && P.a_original && P.m > 0) {
+        // Row activities from the unscaled row-wise copy: each row lists its entries in ascending column order, so
+        // its sequential sum adds the same products in the same order as the column sweep below (explicit zeros
+        // add nothing for finite x). Rows are split over threads; the maximum does not depend on the split.
+        const int nt = std::max(1, std::min(host_threads(), P.m / 4096));
+        std::vector<double> part(size_t(nt), 0.0);
+        auto work = [&](int q) {
+            const int i0 = int(int64_t(P.m) * q / nt), i1 = int(int64_t(P.m) * (q + 1) / nt);
+            double v = 0;
+            for (int i = i0; i < i1; ++i) {
+                double a = 0.0;
+                for (int64_t k = P.A.ptr[i]; k < P.A.ptr[i + 1]; ++k) a += P.A.val[k] * f.x[P.A.idx[k]];
+                v = std::max(v, std::max(md.row_lo[i] - a, a - md.row_up[i]));
+            }
+            part[q] = v;
+        };
+        std::vector<std::thread> pool;
+        for (int q = 1; q < nt; ++q) pool.emplace_back(work, q);
+        work(0);
+        for (auto& th : pool) th.join();
+        for (double v : part) rviol = std::max(rviol, v);
+    } else {
+        std::vector<double> ax(size_t(P.m), 0.0);
+        for (int j = 0; j < P.n; ++j)
+            for (int64_t k = md.col_ptr[j]; k < md.col_ptr[j + 1]; ++k) ax[md.row_idx[k]] += md.val[k] * f.x[j];
+        for (int i = 0; i < P.m; ++i) rviol = std::max(rviol, std::max(md.row_lo[i] - ax[i], ax[i] - md.row_up[i]));
+    }
     f.objective = double(obj), f.max_row_violation = rviol, f.max_bound_violation = bviol;
     return f;
 }

@@ -3,6 +3,8 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -106,8 +108,16 @@ int solve_model(const taral_model& md, const Options& o, SolveResult& res, const
     }
     res.solve_s = since(t);
     res.kernel_launches = e->launches;
-    res.fin = finish_point(md, P, res.outcome);
     res.nnz = e->nnz;
+    t = Clock::now();
+    res.fin = finish_point(md, P, res.outcome);
+    const double finish_s = since(t);
+    t = Clock::now();
+    e.reset();  // device buffers, graph and stream released here rather than at scope exit, so they can be timed
+    const double release_s = since(t);
+    if (std::getenv("TARAL_TIMING"))
+        std::fprintf(stderr, "taral: scale %.4f s, transfer %.4f s, solve %.4f s, finish %.4f s, release %.4f s\n",
+                     res.scale_s, res.transfer_s, res.solve_s, finish_s, release_s);
     res.m = P.m, res.n = P.n;
     return TARAL_OK;
 }

@@ -426,17 +426,32 @@ class RefineryBase:
         (None: all ones). The links of the last period to a later one are dropped."""
         R, Cn = REF_ROWS, REF_COLS
         m, n = periods * R, periods * Cn
-        keep = (self.cols < n) & (self.rows < m)
-        cols, rows, vals = self.cols[keep], self.rows[keep], self.vals[keep]
-        col_ptr = np.zeros(n + 1, np.int64)
-        np.cumsum(np.bincount(cols, minlength=n), out=col_ptr[1:])
+        st = self._structure(periods)
         p = np.ones(2 * REF_GROUPS) if perturb is None else np.asarray(perturb, np.float64)
         fprice = p[self.price_group[:n]]
         fcap_c = p[REF_GROUPS + self.cap_group_col[:n]]
         fcap_r = p[REF_GROUPS + self.cap_group_row[:m]]
+        ax0, rtype = st["ax0"], st["rtype"]
+        row_up = np.where(rtype == 0, ax0, np.where(rtype == 1, (1.3 * ax0 + 10) * fcap_r, INF))
+        return LP(name=name or f"REFINERY_T{periods}", m=m, n=n, col_ptr=st["col_ptr"], row_idx=st["rows"],
+                  val=st["vals"], cost=_r12(self.price[:n] * fprice), col_lo=np.zeros(n),
+                  col_up=_r12(self.cap[:n] * fcap_c), row_lo=st["row_lo"], row_up=_r12(row_up),
+                  row_types=st["row_types"], x_star=self.x0[:n])
+
+    def _structure(self, periods: int) -> dict:
+        """The parts of instance(periods) that the perturbation does not touch (computed once per period count;
+        the arrays are shared by the instances and must not be modified)."""
+        cache = self.__dict__.setdefault("_cache", {})
+        if periods in cache:
+            return cache[periods]
+        R, Cn = REF_ROWS, REF_COLS
+        m, n = periods * R, periods * Cn
+        keep = (self.cols < n) & (self.rows < m)
+        cols, rows, vals = self.cols[keep], self.rows[keep], self.vals[keep]
+        col_ptr = np.zeros(n + 1, np.int64)
+        np.cumsum(np.bincount(cols, minlength=n), out=col_ptr[1:])
         x0 = self.x0[:n]
-        ax0 = np.zeros(m)
-        np.add.at(ax0, rows, vals * x0[cols])
+        ax0 = np.bincount(rows, weights=vals * x0[cols], minlength=m)  # sequential adds in entry order
         rtype = np.empty(m, np.int8)
         loc = np.arange(m) % R
         rtype[loc < 500] = 0                      # E yield
@@ -444,11 +459,12 @@ class RefineryBase:
         rtype[(loc >= 800) & (loc < 1300)] = 2    # G quality
         rtype[loc >= 1300] = 0                    # E inventory
         row_lo = np.where(rtype == 0, ax0, np.where(rtype == 2, ax0 - self.qslack[:m] * (1 + np.abs(ax0)), -INF))
-        row_up = np.where(rtype == 0, ax0, np.where(rtype == 1, (1.3 * ax0 + 10) * fcap_r, INF))
-        return LP(name=name or f"REFINERY_T{periods}", m=m, n=n, col_ptr=col_ptr, row_idx=rows, val=vals,
-                  cost=_r12(self.price[:n] * fprice), col_lo=np.zeros(n), col_up=_r12(self.cap[:n] * fcap_c),
-                  row_lo=_r12(row_lo), row_up=_r12(row_up),
-                  row_types=["E" if k == 0 else ("L" if k == 1 else "G") for k in rtype], x_star=x0)
+        for a in (col_ptr, rows, vals):
+            a.setflags(write=False)
+        st = {"col_ptr": col_ptr, "rows": rows, "vals": vals, "ax0": ax0, "rtype": rtype, "row_lo": _r12(row_lo),
+              "row_types": ["E" if k == 0 else ("L" if k == 1 else "G") for k in rtype]}
+        cache[periods] = st
+        return st
 
 
 def refinery(periods: int = 48, seed: int = 7, perturb: Optional[np.ndarray] = None) -> LP:

@@ -93,14 +93,16 @@ class WarmStart:
         return xs, ys, np.array(ws)
 
 
-def train(P: np.ndarray, X: List[np.ndarray], Y: List[np.ndarray], W: np.ndarray, hidden=512, depth=3, epochs=200,
-          batch=256, lr=1e-3, seed=0) -> WarmStart:
-    """Fit the network to (x, y, log w) of solved scenarios (W: their final primal weights)."""
+def train(P: np.ndarray, X: List[np.ndarray], Y: List[np.ndarray], W: np.ndarray, hidden=512, depth=3, epochs=400,
+          batch=64, lr=3e-4, seed=0) -> WarmStart:
+    """Fit the network to (x, y, log w) of solved scenarios (W: their final primal weights). The output layer
+    starts at zero, so the untrained network predicts the training mean and training can only move away from it
+    where the data supports that."""
     T = np.hstack([np.vstack(X), np.vstack(Y), np.log(np.asarray(W, np.float64))[:, None]])
     norm = Normalizer.fit(T)
     batch = min(batch, len(P))
     net = pdhg.Mlp(P.shape[1], hidden, depth, T.shape[1], max_batch=batch)
-    net.init(seed)
+    net.init(seed, out_scale=0.0)
     net.set_dataset(features(P), norm.encode(T))
     net.last_loss = net.train(epochs=epochs, batch=batch, lr=lr, seed=seed)
     return WarmStart(net, norm, X[0].size, Y[0].size)

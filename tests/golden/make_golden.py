@@ -10,8 +10,11 @@ Needs the reference checkout (REF, default /root/reference) and the reference bi
 * reference_runs.json    reference `pdhg --device cpu --threads 1` (FP64) reports on generated models
 * reference_vectors.npz  the .sol / .dual vectors of those runs
 * reference_optima.json  the reference IPM optimum (`taral --method ipm`) of the planted 2000 x 5000 model
+* reference_bench_lp.json (with --bench-lp, minutes of CPU) the reference `pdhg --device cpu` FP64 report on the
+                         benchmark LP (planted, Zipf rows, 200,000 x 500,000, seed 0) solved to 1e-6: the FP64
+                         iteration count the benchmark's CPU baselines are projected to
 
-Run from the repository root: python tests/golden/make_golden.py
+Run from the repository root: python tests/golden/make_golden.py [--bench-lp]
 """
 import csv
 import hashlib
@@ -115,5 +118,28 @@ def main():
     print("wrote", sorted(p.name for p in OUT.iterdir()))
 
 
+def bench_lp():
+    if not PDHG.exists():
+        sys.exit("build the reference first: make -C oracle ref")
+    sys.path.insert(0, str(ROOT))
+    import bench  # the benchmark's workload definition
+    lp = bench.make_lp(0)
+    threads = os.cpu_count() or 1
+    with tempfile.TemporaryDirectory() as td:
+        f, j = Path(td) / "b.mps", Path(td) / "b.json"
+        lp.write_mps(f)
+        subprocess.run([str(PDHG), str(f), "--device", "cpu", "--threads", str(threads), "--tol", "1e-6", "--json",
+                        str(j)], check=True, stdout=subprocess.DEVNULL)
+        rep = json.loads(j.read_text())
+    out = {"workload": bench.WORKLOAD_NAME, "seed": 0, "model_sha256": lp.digest(), "threads": threads,
+           **{k: rep[k] for k in ("status", "objective", "iterations", "restarts", "rel_primal", "rel_dual", "rel_gap",
+                                  "scale_s", "power_iter_s", "solve_s", "rows", "cols", "nnz")}}
+    (OUT / "reference_bench_lp.json").write_text(json.dumps(out, indent=1) + "\n")
+    print("wrote reference_bench_lp.json:", out["status"], out["iterations"])
+
+
 if __name__ == "__main__":
-    main()
+    if "--bench-lp" in sys.argv:
+        bench_lp()
+    else:
+        main()

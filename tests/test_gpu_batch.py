@@ -77,3 +77,21 @@ def test_batch_deterministic(engine_lib):
     r2, x2, _ = b.solve()
     assert [r["iterations"] for r in r1] == [r["iterations"] for r in r2]
     assert all(np.array_equal(a, c) for a, c in zip(x1, x2))
+
+
+@pytest.mark.parametrize("width", ["1", "8"])
+def test_batch_packs_match_single_solves(engine_lib, monkeypatch, width):
+    # 11 scenarios of one matrix and 2 of another; with packs of up to 8 slots: a pack of 8, a pack of 4 with one
+    # unused slot, a pack of 2. Each batched instance takes the iterates of the same LP solved alone.
+    monkeypatch.setenv("TARAL_BATCH_PACK", width)
+    base = lpgen.RefineryBase(2, seed=5)
+    pert = lpgen.perturbations(13, seed=8)
+    lps = [base.instance(2, p) for p in pert[:11]] + [base.instance(1, p) for p in pert[11:]]
+    b = pdhg.Batch(lps, tol=1e-6, precision=pdhg.FP32, time_limit=300)
+    assert b.info()["distinct_matrices"] == 2
+    res, xs, _ = b.solve()
+    for lp, r, x in zip(lps, res, xs):
+        s, xsol, _ = pdhg.solve(lp, tol=1e-6, precision=pdhg.FP32, time_limit=120)
+        assert r["status"] == "near_optimal" and r["iterations"] == s["iterations"], (lp.name, r["iterations"], s["iterations"])
+        assert rel(r["objective"], s["objective"]) < 1e-9
+        assert np.max(np.abs(x - xsol)) <= 1e-9 * (1 + np.max(np.abs(xsol)))
