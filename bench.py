@@ -21,6 +21,7 @@ the timed region, and the number of engine kernels launched in it.
   python bench.py --impl reference ...                       the reference CPU PDHG (oracle/_ref/pdhg)
   python bench.py --profile-blocks B                         ncu capture mode: B blocks of 64 steps, no report
   python bench.py --workload family [--instances 512]        the batched scenario family against the plain engine
+  python bench.py --workload family --profile-blocks B       ncu capture mode of the batched engine (16 scenarios)
   python bench.py --workload warmstart [--train 512]         the learned warm start on the 24-period family
 """
 import argparse
@@ -324,6 +325,19 @@ def family_lps(count, seed=2024):
     return [base.instance(int(T), p) for T, p in zip(periods, P)], periods
 
 
+def family_profile(args):
+    """ncu capture mode of the batched engine: 16 scenarios of the family structure (8 of 20 periods, 8 of 24
+    periods: two distinct matrices), `--profile-blocks` blocks of 64 iterations, no report."""
+    import lpgen
+    import pdhg
+    base = lpgen.RefineryBase(24, seed=7)
+    P = lpgen.perturbations(16, seed=5)
+    lps = [base.instance(24 if i % 2 else 20, p) for i, p in enumerate(P)]
+    b = pdhg.Batch(lps, tol=WORKLOAD["tol"], precision=pdhg.FP32, max_iter=64 * max(args.profile_blocks, 1))
+    res, _, _ = b.solve(want_points=False)
+    print("profiled", len(res), "scenarios,", res[0]["iterations"], "iterations")
+
+
 def family_arm(args):
     """All scenarios in one batched context (FP32 iterates, FP64 per-instance restart state) against the plain
     single-instance FP32 engine on a stratified sample of them; the plain per-LP time of the whole family is the
@@ -444,7 +458,10 @@ def main():
         return
     if args.workload in ("family", "warmstart"):
         if rank == 0:
-            (family_arm if args.workload == "family" else warmstart_arm)(args)
+            if args.workload == "family" and args.profile_blocks:
+                family_profile(args)
+            else:
+                (family_arm if args.workload == "family" else warmstart_arm)(args)
         return
     if dist:
         import datetime

@@ -158,7 +158,7 @@ __global__ void __launch_bounds__(kThreads, 6) k_pack_spmv(const int* __restrict
     // 2. sums: an item of at most kShort nonzeros by its own thread, longer ones by a warp each
     if (mine) {
         const int rl = tid >> lw, a = sm.rptr[rl], b = sm.rptr[rl + 1];
-        if (b - a <= kShort) {
+        if (b - a <= ((meta.y & kUniformRows) ? kTile : kShort)) {
             double s = 0;
             int k = a;
             for (; k + 8 <= b; k += 8) {  // eight loads in flight, then the adds in entry order
@@ -184,131 +184,6 @@ __global__ void __launch_bounds__(kThreads, 6) k_pack_spmv(const int* __restrict
     }
     __syncthreads();
     if (mine) epi.apply(vbase + tid, sm.rowsum[tid], ops);
-}
-
-// ---------------------------------------------------------------------------------------------- instance groups
-// Width-1 packs that share a matrix form GROUPS of up to kGroup instances. One CTA takes one row block of the shared
-// matrix for a whole group: the block's column indices and values are staged in shared memory once (16-byte loads),
-// then for each live instance in turn the CTA runs block_sums' sequence from the staged copy -- every thread's
-// gathers, the products into shared memory, a thread per row up to kShort nonzeros and a warp per longer row, the
-// fused epilogue -- so each instance gets exactly the single-instance kernel's sums, and the matrix block crosses
-// from L2 once per group instead of once per instance.
-// gext[kGroup * group + t] = {instance, row shift, gather offset, 0} of member t (instance -1: unused slot).
-constexpr int kGroup = 16;
-
-template <class T>
-struct GroupSmem {
-    int idx[kTile + 4];
-    T val[kTile + 4];
-};
-
-template <class T, class X, class E>
-__global__ void __launch_bounds__(kThreads, 6) k_group_spmv(const int* __restrict__ ptr, const int* __restrict__ idx,
-                                                           const T* __restrict__ val, const X* __restrict__ xin,
-                                                           const int4* __restrict__ blk, const int* __restrict__ grp,
-                                                           const int4* __restrict__ gext,
-                                                           const int* __restrict__ active, E epi) {
-    using P = typename ProdT<T, X>::type;
-    __shared__ RowSmem<P> sm;
-    __shared__ GroupSmem<T> gs;
-    const int g = __ldg(grp + blockIdx.x), tid = threadIdx.x;
-    int live_mask = 0;
-    for (int t = 0; t < kGroup; ++t) {
-        const int inst = __ldg(&gext[kGroup * g + t].x);
-        if (inst >= 0 && active[inst]) live_mask |= 1 << t;
-    }
-    if (!live_mask) return;  // uniform: every thread reads the same flags
-    const int4 meta = __ldg(blk + blockIdx.x);
-    const int r0 = meta.x, nrows = meta.y & 0xffff, p0 = meta.z, p1 = meta.w, len = p1 - p0;
-    const bool mine = tid < nrows;
-    if (len > kTile) {  // one long row: block_sums reads it from global memory for each instance
-        for (int t = 0; t < kGroup; ++t) {
-            if (!(live_mask >> t & 1)) continue;
-            const int4 e4 = __ldg(gext + kGroup * g + t);
-            typename E::Ops ops{};
-            if (mine) ops = epi.load(r0 + e4.y + tid, e4.x);
-            block_sums<T, X, true>(ptr, idx, val, xin + e4.z, meta, sm);
-            if (mine) epi.apply(r0 + e4.y + tid, sm.rowsum[tid], ops);
-            __syncthreads();
-        }
-        return;
-    }
-    // stage the block: quads from a0 = p0 & ~3, entry k at k - a0
-    const int a0 = p0 & ~3;
-    for (int q = a0 + 4 * tid; q < p1; q += 4 * kThreads) {
-        if (q >= p0 && q + 4 <= p1) {
-            T v[4];
-            int c[4];
-            Quad<T>::load(val + q, v), load_idx4(idx + q, c);
-#pragma unroll
-            for (int e = 0; e < 4; ++e) gs.val[q - a0 + e] = v[e], gs.idx[q - a0 + e] = c[e];
-        } else {
-#pragma unroll
-            for (int e = 0; e < 4; ++e)
-                if (q + e >= p0 && q + e < p1) gs.val[q - a0 + e] = __ldg(val + q + e), gs.idx[q - a0 + e] = __ldg(idx + q + e);
-        }
-    }
-    for (int t = tid; t <= nrows; t += kThreads) sm.rptr[t] = ptr[r0 + t] - p0;
-    __syncthreads();
-    const int lane = tid & 31, warp = tid >> 5;
-    for (int t = 0; t < kGroup; ++t) {
-        if (!(live_mask >> t & 1)) continue;
-        const int4 e4 = __ldg(gext + kGroup * g + t);
-        const X* xg = xin + e4.z;
-        typename E::Ops ops{};
-        if (mine) ops = epi.load(r0 + e4.y + tid, e4.x);
-        if (tid == 0) sm.nlong = 0;
-        // products: the same (thread, quad) assignment and rounding as block_sums
-        X gv[kQuads][4];
-        int c[kQuads][4];
-#pragma unroll
-        for (int i = 0; i < kQuads; ++i) {
-            const int q = a0 + 4 * (tid + i * kThreads);
-#pragma unroll
-            for (int e = 0; e < 4; ++e) c[i][e] = (q + e >= p0 && q + e < p1) ? gs.idx[q + e - a0] : -1;
-        }
-#pragma unroll
-        for (int i = 0; i < kQuads; ++i)
-#pragma unroll
-            for (int e = 0; e < 4; ++e) gv[i][e] = c[i][e] >= 0 ? gather(xg + c[i][e]) : X(0);
-#pragma unroll
-        for (int i = 0; i < kQuads; ++i) {
-            const int q = a0 + 4 * (tid + i * kThreads);
-#pragma unroll
-            for (int e = 0; e < 4; ++e)
-                if (c[i][e] >= 0) sm.prod[pidx(q + e - p0)] = P(gs.val[q + e - a0]) * P(gv[i][e]);
-        }
-        __syncthreads();
-        if (mine) {
-            const int a = sm.rptr[tid], b = sm.rptr[tid + 1];
-            if (b - a <= kShort) {
-                double s = 0;
-                int k = a;
-                for (; k + 4 <= b; k += 4) {
-                    P tt[4];
-#pragma unroll
-                    for (int e = 0; e < 4; ++e) tt[e] = sm.prod[pidx(k + e)];
-#pragma unroll
-                    for (int e = 0; e < 4; ++e) s += double(tt[e]);
-                }
-                for (; k < b; ++k) s += double(sm.prod[pidx(k)]);
-                sm.rowsum[tid] = s;
-            } else {
-                sm.longrow[atomicAdd(&sm.nlong, 1)] = short(tid);
-            }
-        }
-        __syncthreads();
-        for (int i = warp; i < sm.nlong; i += kThreads / 32) {
-            const int r = sm.longrow[i];
-            double s = 0;
-            for (int k = sm.rptr[r] + lane; k < sm.rptr[r + 1]; k += 32) s += double(sm.prod[pidx(k)]);
-            for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
-            if (lane == 0) sm.rowsum[r] = s;
-        }
-        __syncthreads();
-        if (mine) epi.apply(r0 + e4.y + tid, sm.rowsum[tid], ops);
-        __syncthreads();  // the next member reuses the product and row-sum arrays
-    }
 }
 
 // Per-(CTA, slot) partial sums of the row (ROW = true) or column KKT scalars over one pack block, CTAs in
@@ -633,9 +508,6 @@ template <class T>
 struct Batch final : BatchBase {
     int ninst = 0, M = 0, N = 0, nA = 0, nT = 0, freq = 64;
     int nA1 = 0, nT1 = 0, nAp = 0, nTp = 0;  // iteration CTAs: width-1 packs (k_rowblock_batch), wider packs
-    int nAg = 0, nTg = 0;                     // iteration CTAs of instance groups (k_group_spmv)
-    int *A_grp = nullptr, *T_grp = nullptr;
-    int4 *A_git = nullptr, *T_git = nullptr, *gextA = nullptr, *gextT = nullptr;
     Options opt;
     std::vector<const taral_model*> models;
     std::vector<int> mat_of;                 // instance -> distinct matrix
@@ -881,36 +753,10 @@ struct Batch final : BatchBase {
         // run on the single-instance skeleton k_rowblock_batch, whose block extension is {instance, row shift,
         // gather offset, 0}; wider packs on k_pack_spmv.
         std::vector<int4> a1_it, ae1_it, t1_it, te1_it;
-        bool grouping = false;  // TARAL_BATCH_GROUP=1: one CTA per (block, group of instances) instead of per instance
-        if (const char* e = std::getenv("TARAL_BATCH_GROUP")) grouping = std::atoi(e) != 0;
-        std::vector<int4> ga_it, gt_it, hgA, hgT;
-        std::vector<int> ga_grp, gt_grp;
-        for (int k = 0; k < distinct && grouping; ++k) {
-            const Shared& sh = *mats[k];
-            std::vector<int> ones;
-            for (int p : packs_of[k])
-                if (packs[p].W == 1) ones.push_back(p);
-            if (ones.empty()) continue;
-            const auto& bl = sh.blk.at(1);
-            for (size_t g0 = 0; g0 < ones.size(); g0 += kGroup) {
-                const int gid = int(hgA.size() / kGroup);
-                for (int t = 0; t < kGroup; ++t) {
-                    const bool in = g0 + t < ones.size();
-                    const Pack& q = packs[in ? ones[g0 + t] : ones[0]];
-                    hgA.push_back(in ? make_int4(q.inst[0], q.rbase - sh.pbaseA, q.cbase, 0) : make_int4(-1, 0, 0, 0));
-                    hgT.push_back(in ? make_int4(q.inst[0], q.cbase - sh.pbaseT, q.rbase, 0) : make_int4(-1, 0, 0, 0));
-                }
-                for (const int4& b : bl.first) ga_it.push_back(rebase(b, sh.pbaseA, sh.nnzbase)), ga_grp.push_back(gid);
-                for (const int4& b : bl.second) gt_it.push_back(rebase(b, sh.pbaseT, sh.nnzbase)), gt_grp.push_back(gid);
-            }
-        }
-        nAg = int(ga_it.size()), nTg = int(gt_it.size());
-        A_git = put(ga_it), T_git = put(gt_it), A_grp = put(ga_grp), T_grp = put(gt_grp), gextA = put(hgA), gextT = put(hgT);
         for (int k = 0; k < distinct; ++k) {
             const Shared& sh = *mats[k];
             for (const auto& wb : sh.blk) {
                 const bool one = wb.first == 1;
-                if (one && grouping) continue;  // served by the groups
                 for (const int4& b : wb.second.first)
                     for (int p : packs_of[k]) {
                         if (packs[p].W != wb.first) continue;
@@ -972,13 +818,11 @@ struct Batch final : BatchBase {
     // ------------------------------------------------------------------ launches
     template <class X, class E>
     void spmv_A(const X* xin, const E& e, const int* act) {
-        if (nAg) k_group_spmv<T, X, E><<<nAg, kThreads, 0, s>>>(Aptr, Aidx, Aval, xin, A_git, A_grp, gextA, act, e), ++launches;
         if (nA1) k_rowblock_batch<T, X, E, true><<<nA1, kThreads, 0, s>>>(Aptr, Aidx, Aval, xin, A1_it, Ae1_it, act, e), ++launches;
         if (nAp) k_pack_spmv<T, X, E><<<nAp, kThreads, 0, s>>>(Aptr, Aidx, Aval, xin, A_it, Ae_it, slot_inst, act, e), ++launches;
     }
     template <class X, class E>
     void spmv_T(const X* xin, const E& e, const int* act) {
-        if (nTg) k_group_spmv<T, X, E><<<nTg, kThreads, 0, s>>>(Tptr, Tidx, Tval, xin, T_git, T_grp, gextT, act, e), ++launches;
         if (nT1) k_rowblock_batch<T, X, E, true><<<nT1, kThreads, 0, s>>>(Tptr, Tidx, Tval, xin, T1_it, Te1_it, act, e), ++launches;
         if (nTp) k_pack_spmv<T, X, E><<<nTp, kThreads, 0, s>>>(Tptr, Tidx, Tval, xin, T_it, Te_it, slot_inst, act, e), ++launches;
     }
@@ -1167,7 +1011,9 @@ struct Batch final : BatchBase {
         BK(cudaEventElapsedTime(&ms, e0, e1));
         cudaEventDestroy(e0), cudaEventDestroy(e1);
         double solve_s = since(t0);
-        for (int i = 0; i < ninst; ++i) {
+        // original-space check of every instance (independent: spread over the host threads)
+        std::atomic<int> next{0};
+        auto finish_one = [&](int i) {
             const InstState& q = fin[i];
             const Shared& sh = *mats[mat_of[i]];
             Outcome r;
@@ -1189,7 +1035,14 @@ struct Batch final : BatchBase {
             o.device_s = ms * 1e-3;
             if (xo && xo[i]) std::memcpy(xo[i], f.x.data(), f.x.size() * sizeof(double));
             if (yo && yo[i]) std::memcpy(yo[i], f.y.data(), f.y.size() * sizeof(double));
-        }
+        };
+        std::vector<std::thread> pool;
+        const int nt = std::max(1, std::min(host_threads(), ninst));
+        for (int t = 0; t < nt; ++t)
+            pool.emplace_back([&] {
+                for (int i = next++; i < ninst; i = next++) finish_one(i);
+            });
+        for (auto& th : pool) th.join();
     }
     int64_t per_graph = 0;
 };

@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdarg>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -35,7 +36,14 @@ std::vector<int4> build_row_blocks(const int64_t* ptr, int rows) { return build_
 
 std::vector<int4> build_row_blocks(const int64_t* ptr, int rows, int tile, int rows_max) {
     std::vector<int4> out;
-    auto close = [&](int r0, int r1) { out.push_back(make_int4(r0, r1 - r0, int(ptr[r0]), int(ptr[r1]))); };
+    auto close = [&](int r0, int r1) {  // y: rows | kUniformRows when no row is much longer than the block's mean
+        int64_t mx = 0;
+        for (int r = r0; r < r1; ++r) mx = std::max<int64_t>(mx, ptr[r + 1] - ptr[r]);
+        const int64_t nz = ptr[r1] - ptr[r0], mean = (nz + (r1 - r0) - 1) / (r1 - r0);
+        static const bool on = std::getenv("TARAL_UNIFORM") != nullptr;  // temporary A/B switch
+        const bool uniform = on && r1 - r0 > 1 && mx > kShort && mx <= 2 * mean + 8;
+        out.push_back(make_int4(r0, (r1 - r0) | (uniform ? kUniformRows : 0), int(ptr[r0]), int(ptr[r1])));
+    };
     int start = 0, cur_rows = 0;
     int64_t cur_nnz = 0;
     for (int r = 0; r < rows; ++r) {

@@ -126,6 +126,10 @@ struct EpiCol {
 // Row-block metadata, one int4 per block, built on the host (build_row_blocks): x = first row, y = number of rows,
 // z = first nonzero, w = end of the nonzeros. VEC: the val/idx base pointers are 16-byte aligned.
 constexpr int kShort = 48;                       // rows up to this length are summed by their own thread
+// Block flag (bit 16 of the metadata's row count): the block's rows have similar lengths (longest <= 2 x mean + 8),
+// so every row, however long, is summed by its own thread in entry order -- the warp path only pays off when a few
+// long rows would otherwise hold up a warp of short ones.
+constexpr int kUniformRows = 1 << 16;
 constexpr int kQuads = (kTile + 3 + 3) / 4 / kThreads;  // 16-byte quads per thread in the staging loop (2)
 static_assert(kQuads * 4 * kThreads >= kTile + 3, "a block's quads must fit the staging loop");
 __device__ __forceinline__ int pidx(int k) { return k + (k >> 5); }  // one pad slot per 32: no bank conflicts
@@ -218,10 +222,11 @@ __device__ __forceinline__ void block_sums(const int* __restrict__ ptr, const in
     }
     __syncthreads();
 
-    // 2. reduce: short rows by their own thread, long rows by a warp each
+    // 2. reduce: short rows (every row of a uniform block) by their own thread, long rows by a warp each
+    const int thread_max = (meta.y & kUniformRows) ? kTile : kShort;
     if (tid < nrows) {
         const int a = sm.rptr[tid], b = sm.rptr[tid + 1];
-        if (b - a <= kShort) {
+        if (b - a <= thread_max) {
             double s = 0;
             int k = a;
             for (; k + 4 <= b; k += 4) {  // four loads in flight, then the adds in entry order

@@ -12,6 +12,8 @@
 #include <fstream>
 #include <map>
 #include <sstream>
+#include <charconv>
+#include <string_view>
 #include <unordered_map>
 #include <unordered_set>
 
@@ -22,7 +24,7 @@ namespace {
 
 constexpr double kHuge = 1e20;  // |bound| >= 1e20 is infinite
 
-double parse_number(const std::string& s) {
+double parse_number(std::string_view s) {
     size_t i = 0, n = s.size();
     auto digits = [&] {
         size_t a = i;
@@ -38,24 +40,32 @@ double parse_number(const std::string& s) {
         if (i < n && (s[i] == '+' || s[i] == '-')) ++i;
         ok = digits() > 0;
     }
-    if (!ok || i != n) throw ParseError("bad number '" + s + "'");
-    std::string t = s;
-    for (char& ch : t)
-        if (ch == 'd' || ch == 'D') ch = 'E';
-    double v = std::strtod(t.c_str(), nullptr);
-    if (!std::isfinite(v)) throw ParseError("number '" + s + "' is not finite");
+    if (!ok || i != n) throw ParseError("bad number '" + std::string(s) + "'");
+    char small[96];
+    std::string big;
+    char* t = small;
+    if (n + 1 > sizeof small) big.resize(n + 1), t = &big[0];
+    for (size_t k = 0; k < n; ++k) t[k] = (s[k] == 'd' || s[k] == 'D') ? 'E' : s[k];
+    t[n] = 0;
+    // from_chars rounds correctly like strtod (the same double); out-of-range text goes to strtod, whose overflow /
+    // underflow results the checks below and the callers expect
+    double v = 0;
+    const auto r = std::from_chars(t, t + n, v);
+    if (r.ec != std::errc() || r.ptr != t + n) v = std::strtod(t, nullptr);
+    if (!std::isfinite(v)) throw ParseError("number '" + std::string(s) + "' is not finite");
     return v;
 }
 
-std::string fixed_field(const std::string& line, size_t a, size_t b) {
-    if (line.size() <= a) return "";
-    std::string s = line.substr(a, b - a);
+std::string_view fixed_field(std::string_view line, size_t a, size_t b) {
+    if (line.size() <= a) return {};
+    std::string_view s = line.substr(a, b - a);
     size_t i = s.find_first_not_of(" \t"), j = s.find_last_not_of(" \t\r");
-    return i == std::string::npos ? "" : s.substr(i, j - i + 1);
+    return i == std::string_view::npos ? std::string_view() : s.substr(i, j - i + 1);
 }
 
-std::vector<std::string> split(const std::string& line, const std::string& section, bool fixed) {
-    std::vector<std::string> t;
+// Tokens of one data line (views into the line): whitespace-separated (free format) or the fixed-column fields.
+void split(std::string_view line, const std::string& section, bool fixed, std::vector<std::string_view>& t) {
+    t.clear();
     if (!fixed) {
         auto ws = [](char c) { return c == ' ' || c == '\t' || c == '\n' || c == '\v' || c == '\f' || c == '\r'; };
         size_t p = 0, e = line.size();
@@ -63,9 +73,9 @@ std::vector<std::string> split(const std::string& line, const std::string& secti
             while (p < e && ws(line[p])) ++p;
             size_t s = p;
             while (p < e && !ws(line[p])) ++p;
-            if (p > s) t.emplace_back(line, s, p - s);
+            if (p > s) t.push_back(line.substr(s, p - s));
         }
-        return t;
+        return;
     }
     auto f = [&](size_t a, size_t b) { t.push_back(fixed_field(line, a, b)); };
     if (section == "ROWS") {
@@ -77,7 +87,6 @@ std::vector<std::string> split(const std::string& line, const std::string& secti
         f(4, 12), f(14, 22), f(24, 36);
         if (!fixed_field(line, 39, 47).empty()) f(39, 47), f(49, 61);
     }
-    return t;
 }
 
 struct Entry {
@@ -85,21 +94,85 @@ struct Entry {
     double v;
 };
 
-Model parse(const std::string& path, bool fixed) {
-    std::ifstream in(path);
+// Name -> index for the ROWS and COLUMNS names: open addressing with linear probing over views into the file
+// buffer (the buffer outlives the table), 64-bit FNV-1a hashes kept per slot, grown at half load.
+class NameTable {
+  public:
+    explicit NameTable(size_t expect) { rehash(std::max<size_t>(64, next_pow2(2 * expect))); }
+    const int* find(std::string_view k) const {
+        const uint64_t h = hash(k);
+        for (size_t i = h & mask_;; i = (i + 1) & mask_) {
+            if (idx_[i] < 0) return nullptr;
+            if (hash_[i] == h && key_[i] == k) return &idx_[i];
+        }
+    }
+    bool count(std::string_view k) const { return find(k) != nullptr; }
+    void insert(std::string_view k, int v) {  // k must not be present
+        if (2 * (n_ + 1) > key_.size()) rehash(2 * key_.size());
+        place(k, hash(k), v);
+        ++n_;
+    }
+
+  private:
+    std::vector<std::string_view> key_;
+    std::vector<uint64_t> hash_;
+    std::vector<int> idx_;
+    size_t mask_ = 0, n_ = 0;
+    static size_t next_pow2(size_t x) {
+        size_t p = 1;
+        while (p < x) p <<= 1;
+        return p;
+    }
+    static uint64_t hash(std::string_view k) {
+        uint64_t h = 1469598103934665603ull;
+        for (unsigned char c : k) h = (h ^ c) * 1099511628211ull;
+        return h ^ (h >> 29);
+    }
+    void place(std::string_view k, uint64_t h, int v) {
+        size_t i = h & mask_;
+        while (idx_[i] >= 0) i = (i + 1) & mask_;
+        key_[i] = k, hash_[i] = h, idx_[i] = v;
+    }
+    void rehash(size_t size) {
+        std::vector<std::string_view> k(std::move(key_));
+        std::vector<uint64_t> h(std::move(hash_));
+        std::vector<int> v(std::move(idx_));
+        key_.assign(size, std::string_view()), hash_.assign(size, 0), idx_.assign(size, -1);
+        mask_ = size - 1;
+        for (size_t i = 0; i < v.size(); ++i)
+            if (v[i] >= 0) place(k[i], h[i], v[i]);
+    }
+};
+
+std::string read_file(const std::string& path) {
+    std::ifstream in(path, std::ios::binary);
     if (!in) throw ParseError("cannot open " + path);
+    in.seekg(0, std::ios::end);
+    const std::streamoff size = in.tellg();
+    in.seekg(0, std::ios::beg);
+    std::string buf(size > 0 ? size_t(size) : 0, '\0');
+    if (size > 0 && !in.read(&buf[0], size)) throw ParseError("cannot read " + path);
+    return buf;
+}
+
+// Row / column names are views into the file buffer, which outlives the parse.
+Model parse(const std::string& path, bool fixed) {
+    const std::string buf = read_file(path);
     Model md;
-    std::string section, obj_row, line;
-    std::unordered_map<std::string, int> row_id, col_id;
-    std::unordered_set<std::string> free_rows, seen;
+    std::string section, obj_row;
+    NameTable row_id(buf.size() / 512 + 16), col_id(buf.size() / 256 + 16);
+    std::unordered_set<std::string_view> free_rows;
+    std::unordered_set<std::string> seen;
     std::vector<char> row_type;
     std::vector<double> rhs, range;
     std::vector<char> has_range;
     bool in_int = false, endata = false, q_full = false;
     int cur = -1;
+    std::string_view cur_name;
     std::vector<Entry> pending;
     std::string rhs_set, range_set, bound_set;
     std::map<std::pair<int, int>, double> q;
+    std::vector<std::string_view> t;
 
     auto close_column = [&] {  // sorted by row, duplicates summed in file order, zero sums dropped
         if (cur < 0) return;
@@ -116,28 +189,31 @@ Model parse(const std::string& path, bool fixed) {
         md.col_ptr.push_back(int64_t(w));
         pending.clear();
     };
-    auto first_set = [](std::string& keep, const std::string& nm) {
-        if (keep.empty()) keep = nm;
+    auto first_set = [](std::string& keep, std::string_view nm) {
+        if (keep.empty()) keep = std::string(nm);
         return keep == nm;
     };
-    auto row_of = [&](const std::string& nm) -> int {
-        auto it = row_id.find(nm);
-        if (it != row_id.end()) return it->second;
+    auto row_of = [&](std::string_view nm) -> int {
+        if (const int* r = row_id.find(nm)) return *r;
         if (nm == obj_row) return -1;
         if (free_rows.count(nm)) return -2;
-        throw ParseError("unknown row '" + nm + "'");
+        throw ParseError("unknown row '" + std::string(nm) + "'");
     };
-    auto col_of = [&](const std::string& nm) {
-        auto it = col_id.find(nm);
-        if (it == col_id.end()) throw ParseError("unknown column '" + nm + "'");
-        return it->second;
+    auto col_of = [&](std::string_view nm) {
+        const int* c = col_id.find(nm);
+        if (!c) throw ParseError("unknown column '" + std::string(nm) + "'");
+        return *c;
     };
 
-    while (std::getline(in, line)) {
-        if (!line.empty() && line.back() == '\r') line.pop_back();
-        if (line.find_first_not_of(" \t") == std::string::npos || line[0] == '*') continue;
+    for (size_t pos = 0; pos < buf.size();) {
+        size_t nl = buf.find('\n', pos);
+        if (nl == std::string::npos) nl = buf.size();
+        std::string_view line(buf.data() + pos, nl - pos);
+        pos = nl + 1;
+        if (!line.empty() && line.back() == '\r') line.remove_suffix(1);
+        if (line.find_first_not_of(" \t") == std::string_view::npos || line[0] == '*') continue;
         if (line[0] != ' ' && line[0] != '\t') {  // section header
-            std::istringstream hs(line);
+            std::istringstream hs{std::string(line)};
             std::string arg;
             hs >> section >> arg;
             if (section == "NAME") {
@@ -166,45 +242,46 @@ Model parse(const std::string& path, bool fixed) {
                 throw ParseError("section " + section + " appears twice");
             continue;
         }
-        std::vector<std::string> t = split(line, section, fixed);
+        split(line, section, fixed, t);
         if (section == "OBJSENSE") {
-            std::string v = t.empty() ? "" : t[0];
+            std::string_view v = t.empty() ? std::string_view() : t[0];
             if (v == "MAX" || v == "MAXIMIZE") md.maximize = true;
-            else if (v != "MIN" && v != "MINIMIZE") throw ParseError("bad OBJSENSE " + v);
+            else if (v != "MIN" && v != "MINIMIZE") throw ParseError("bad OBJSENSE " + std::string(v));
         } else if (section == "ROWS") {
             if (t.size() != 2 || t[1].empty()) throw ParseError("bad ROWS line");
             char type = t[0].empty() ? '?' : char(std::toupper(static_cast<unsigned char>(t[0][0])));
             if (row_id.count(t[1]) || t[1] == obj_row || free_rows.count(t[1]))
-                throw ParseError("duplicate row name '" + t[1] + "'");
+                throw ParseError("duplicate row name '" + std::string(t[1]) + "'");
             if (type == 'N') {
-                if (obj_row.empty()) obj_row = t[1];
+                if (obj_row.empty()) obj_row = std::string(t[1]);
                 else free_rows.insert(t[1]);
             } else if (type == 'E' || type == 'L' || type == 'G') {
-                row_id[t[1]] = int(md.row_names.size());
-                md.row_names.push_back(t[1]);
+                row_id.insert(t[1], int(md.row_names.size()));
+                md.row_names.emplace_back(t[1]);
                 row_type.push_back(type);
             } else {
-                throw ParseError("bad row type " + t[0]);
+                throw ParseError("bad row type " + std::string(t[0]));
             }
         } else if (section == "COLUMNS") {
             if (t.size() >= 2 && t[1] == "'MARKER'") {
                 bool s = false, e = false;
-                for (const std::string& w : t) s |= w == "'INTORG'", e |= w == "'INTEND'";
+                for (std::string_view w : t) s |= w == "'INTORG'", e |= w == "'INTEND'";
                 if (s == e) throw ParseError("bad MARKER line");
                 in_int = s;
                 continue;
             }
             if (t.size() != 3 && t.size() != 5) throw ParseError("bad COLUMNS line");
             int j;
-            if (cur >= 0 && t[0] == md.col_names[cur]) {
+            if (cur >= 0 && t[0] == cur_name) {
                 j = cur;
             } else {
-                auto it = col_id.find(t[0]);
-                if (it != col_id.end()) throw ParseError("column '" + t[0] + "' is listed in two separate blocks");
+                if (col_id.count(t[0]))
+                    throw ParseError("column '" + std::string(t[0]) + "' is listed in two separate blocks");
                 close_column();
                 j = int(md.col_names.size());
-                col_id[t[0]] = j;
-                md.col_names.push_back(t[0]);
+                col_id.insert(t[0], j);
+                md.col_names.emplace_back(t[0]);
+                cur_name = t[0];
                 md.cost.push_back(0);
                 md.is_int.push_back(in_int ? 1 : 0);
             }
@@ -238,11 +315,12 @@ Model parse(const std::string& path, bool fixed) {
                 md.col_lo.assign(md.col_names.size(), 0);
                 md.col_up.assign(md.col_names.size(), kInf);
             }
-            std::string type = t.empty() ? "" : t[0];
+            std::string_view type = t.empty() ? std::string_view() : t[0];
             bool no_value = type == "FR" || type == "MI" || type == "PL" || type == "BV";
-            std::string set, col, val;
+            std::string_view set, col, val;
             if (fixed) {
-                set = t.size() > 1 ? t[1] : "", col = t.size() > 2 ? t[2] : "", val = t.size() > 3 ? t[3] : "";
+                set = t.size() > 1 ? t[1] : std::string_view(), col = t.size() > 2 ? t[2] : std::string_view();
+                val = t.size() > 3 ? t[3] : std::string_view();
             } else if (t.size() == 4) {
                 set = t[1], col = t[2], val = t[3];
             } else if (t.size() == 3) {
@@ -254,9 +332,9 @@ Model parse(const std::string& path, bool fixed) {
                 throw ParseError("bad BOUNDS line");
             }
             if (!set.empty() && !first_set(bound_set, set)) continue;
-            auto it = col_id.find(col);
-            if (it == col_id.end()) throw ParseError("unknown column '" + col + "' in BOUNDS");
-            int j = it->second;
+            const int* jc = col_id.find(col);
+            if (!jc) throw ParseError("unknown column '" + std::string(col) + "' in BOUNDS");
+            int j = *jc;
             double v = no_value || val.empty() ? 0 : parse_number(val);
             double &lo = md.col_lo[j], &up = md.col_up[j];
             if (type == "BV" || type == "LI" || type == "UI") md.is_int[j] = 1;
@@ -269,7 +347,7 @@ Model parse(const std::string& path, bool fixed) {
             else if (type == "MI") lo = -kInf;
             else if (type == "PL") up = kInf;
             else if (type == "BV") lo = 0, up = 1;
-            else throw ParseError("unsupported bound type " + type);
+            else throw ParseError("unsupported bound type " + std::string(type));
         } else if (section == "QUAD") {
             if (t.size() != 3) throw ParseError("bad quadratic objective line");
             int a = col_of(t[0]), b = col_of(t[1]);
