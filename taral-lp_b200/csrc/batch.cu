@@ -526,6 +526,8 @@ struct Batch final : BatchBase {
     T *Aval = nullptr, *Tval = nullptr;
     int4 *A_it = nullptr, *Ae_it = nullptr, *T_it = nullptr, *Te_it = nullptr;
     int4 *A1_it = nullptr, *Ae1_it = nullptr, *T1_it = nullptr, *Te1_it = nullptr;
+    std::vector<int4> h_a1, h_ap, h_t1, h_tp;  // host copies of the iteration block lists (autotuner)
+    int tuned[2] = {0, 0};
     int4 *A_ev = nullptr, *Ae_ev = nullptr, *T_ev = nullptr, *Te_ev = nullptr;
     int *rr = nullptr, *cr = nullptr, *slot_inst = nullptr;
     int2* d_where = nullptr;
@@ -543,13 +545,16 @@ struct Batch final : BatchBase {
     std::vector<void*> allocs;
 
     template <class U>
-    U* alloc(size_t n) {
+    U* alloc(size_t n) {  // stream-ordered, from the device's memory pool (keep_pool_memory)
         void* p = nullptr;
-        cudaError_t e = cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(U));
+        const size_t bytes = std::max<size_t>(n, 1) * sizeof(U);
+        cudaError_t e = cudaMallocAsync(&p, bytes, s);
         if (e != cudaSuccess) throw BatchError{std::string("cudaMalloc: ") + cudaGetErrorString(e)};
         allocs.push_back(p);
+        alloc_bytes += bytes;
         return static_cast<U*>(p);
     }
+    size_t alloc_bytes = 0;
     template <class U>
     U* put(const std::vector<U>& h) {
         U* p = alloc<U>(h.size());
@@ -559,16 +564,17 @@ struct Batch final : BatchBase {
     }
     ~Batch() override {
         if (graph) cudaGraphExecDestroy(graph);
+        for (void* p : allocs) cudaFreeAsync(p, s);
         if (s) cudaStreamSynchronize(s);
-        for (void* p : allocs) cudaFree(p);
         if (h_count) cudaFreeHost(h_count);
         if (s) cudaStreamDestroy(s);
     }
 
     void build(const taral_model* md, int count, const Options& o) {
         ninst = count, opt = o, freq = std::max(1, o.eval_freq);
-        size_t free0, free1, total;
-        BK(cudaMemGetInfo(&free0, &total));
+        int dev = 0;
+        BK(cudaGetDevice(&dev));
+        keep_pool_memory(dev);
         BK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
         // 1. distinct matrices (same sizes and identical col_ptr / row_idx / val)
         std::map<std::pair<uint64_t, std::pair<int, int>>, int> seen;
@@ -649,11 +655,12 @@ struct Batch final : BatchBase {
         {
             struct Scratch {
                 std::vector<void*> p;
-                ~Scratch() { for (void* q : p) cudaFree(q); }
-            } tmp;
+                cudaStream_t st;
+                ~Scratch() { for (void* q : p) cudaFreeAsync(q, st); }
+            } tmp{{}, s};
             auto scratch = [&](size_t k) {
                 void* q = nullptr;
-                BK(cudaMalloc(&q, std::max<size_t>(k, 1) * sizeof(double)));
+                BK(cudaMallocAsync(&q, std::max<size_t>(k, 1) * sizeof(double), s));
                 tmp.p.push_back(q);
                 return static_cast<double*>(q);
             };
@@ -776,6 +783,7 @@ struct Batch final : BatchBase {
         nA = int(a_ev.size()), nT = int(t_ev.size());
         nA1 = int(a1_it.size()), nT1 = int(t1_it.size()), nAp = int(a_it.size()), nTp = int(t_it.size());
         A1_it = put(a1_it), Ae1_it = put(ae1_it), T1_it = put(t1_it), Te1_it = put(te1_it);
+        h_a1 = a1_it, h_ap = a_it, h_t1 = t1_it, h_tp = t_it;
         slot_inst = put(hslot), d_where = put(where);
         // 5. upload
         A_it = put(a_it), Ae_it = put(ae_it), T_it = put(t_it), Te_it = put(te_it);
@@ -806,12 +814,80 @@ struct Batch final : BatchBase {
         d_deadline = alloc<unsigned long long>(1);
         BK(cudaMallocHost(&h_count, sizeof(int)));
         BK(cudaStreamSynchronize(s));
-        BK(cudaMemGetInfo(&free1, &total));
-        mem_used = free0 - free1;
+        mem_used = alloc_bytes;
         nnz_total = 0;
         for (int i = 0; i < count; ++i) nnz_total += mats[mat_of[i]]->nnz;
         models.clear();
         for (int i = 0; i < count; ++i) models.push_back(md + i);
+        tune();
+    }
+
+    // Row-split autotuner (FP32 batches; the engine's three policies, per phase over the whole batch): a policy other
+    // than the hybrid rule is kept only if it is at least 5 % faster. TARAL_TUNE=0 keeps the hybrid rule.
+    void tune() {
+        if (sizeof(T) != sizeof(float)) return;
+        if (const char* e = std::getenv("TARAL_TUNE"))
+            if (std::atoi(e) == 0) return;
+        int forced = -1;  // TARAL_ROWSPLIT=0|1|2: that policy, untimed
+        if (const char* e = std::getenv("TARAL_ROWSPLIT")) forced = std::max(0, std::min(2, std::atoi(e)));
+        if (forced < 0 && nnz_total < (int64_t(1) << 20)) return;  // small: timings are noise
+        std::vector<int> ones(size_t(ninst), 1);
+        BK(cudaMemcpyAsync(pactive, ones.data(), ones.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+        BK(cudaMemsetAsync(pv, 0, size_t(N) * sizeof(T), s));
+        BK(cudaMemsetAsync(pw, 0, size_t(M) * sizeof(T), s));
+        auto variant = [](const std::vector<int4>& h, int policy, bool& any) {
+            std::vector<int4> a(h);
+            for (int4& b : a) {
+                if (policy == 1 && (b.y & kUniformCandidate)) b.y |= kUniformRows, any = true;
+                if (policy == 2) b.y |= kSegmented, any = true;
+            }
+            return a;
+        };
+        for (int phase = 0; phase < 2; ++phase) {
+            std::vector<int4>& h1 = phase ? h_t1 : h_a1;
+            std::vector<int4>& hp = phase ? h_tp : h_ap;
+            int4* d1 = phase ? T1_it : A1_it;
+            int4* dp = phase ? T_it : A_it;
+            auto put_lists = [&](const std::vector<int4>& l1, const std::vector<int4>& lp) {
+                if (!l1.empty()) BK(cudaMemcpyAsync(d1, l1.data(), l1.size() * sizeof(int4), cudaMemcpyHostToDevice, s));
+                if (!lp.empty()) BK(cudaMemcpyAsync(dp, lp.data(), lp.size() * sizeof(int4), cudaMemcpyHostToDevice, s));
+            };
+            auto run = [&] {
+                if (phase) spmv_T(pw, EpiStore<T>{pu}, pactive);
+                else spmv_A(pv, EpiStore<T>{pw}, pactive);
+            };
+            auto time_lists = [&](const std::vector<int4>& l1, const std::vector<int4>& lp) {
+                put_lists(l1, lp);
+                for (int r = 0; r < 2; ++r) run();
+                cudaEvent_t e0, e1;
+                BK(cudaEventCreate(&e0));
+                BK(cudaEventCreate(&e1));
+                BK(cudaEventRecord(e0, s));
+                for (int r = 0; r < 5; ++r) run();
+                BK(cudaEventRecord(e1, s));
+                BK(cudaEventSynchronize(e1));
+                float ms = 0;
+                BK(cudaEventElapsedTime(&ms, e0, e1));
+                cudaEventDestroy(e0), cudaEventDestroy(e1);
+                return ms;
+            };
+            std::vector<int4> v1[3], vp[3];
+            float t[3] = {0, 1e30f, 1e30f};
+            for (int pol = 0; pol < 3; ++pol) {
+                bool any = pol == 0;
+                v1[pol] = variant(h1, pol, any), vp[pol] = variant(hp, pol, any);
+                if (any && forced < 0) t[pol] = time_lists(v1[pol], vp[pol]);
+            }
+            int best = 0;
+            for (int k = 1; k < 3; ++k)
+                if (t[k] < 0.95f * t[0] && t[k] < t[best]) best = k;
+            if (forced >= 0) best = forced;
+            tuned[phase] = best;
+            h1 = v1[best], hp = vp[best];
+            put_lists(h1, hp);
+            BK(cudaStreamSynchronize(s));
+        }
+        launches = 0;
     }
     std::vector<int> first_inst;  // distinct matrix -> first instance that has it
 

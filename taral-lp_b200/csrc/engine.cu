@@ -18,6 +18,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -29,6 +30,23 @@
 
 namespace taral {
 
+// ---------------------------------------------------------------------------------------------- memory
+// Device buffers come from the device's default memory pool (cudaMallocAsync / cudaFreeAsync on the context's
+// stream). The pool keeps up to 32 GB of freed memory for the process, so a context's release is a stream-ordered
+// return to the pool and the next context of the process reuses the memory without new device allocations.
+void keep_pool_memory(int dev) {
+    static std::mutex mu;
+    static std::vector<int> done;
+    std::lock_guard<std::mutex> lock(mu);
+    if (std::find(done.begin(), done.end(), dev) != done.end()) return;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t keep = uint64_t(32) << 30;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    done.push_back(dev);
+}
+
 // ---------------------------------------------------------------------------------------------- row blocks
 // Consecutive rows are packed into blocks of at most kTile nonzeros and kRowsMax rows; a longer row is a block of
 // its own (block_sums sums it with the whole CTA).
@@ -36,13 +54,12 @@ std::vector<int4> build_row_blocks(const int64_t* ptr, int rows) { return build_
 
 std::vector<int4> build_row_blocks(const int64_t* ptr, int rows, int tile, int rows_max) {
     std::vector<int4> out;
-    auto close = [&](int r0, int r1) {  // y: rows | kUniformRows when no row is much longer than the block's mean
+    auto close = [&](int r0, int r1) {  // y: rows | kUniformCandidate when no row is much longer than the mean
         int64_t mx = 0;
         for (int r = r0; r < r1; ++r) mx = std::max<int64_t>(mx, ptr[r + 1] - ptr[r]);
         const int64_t nz = ptr[r1] - ptr[r0], mean = (nz + (r1 - r0) - 1) / (r1 - r0);
-        static const bool on = std::getenv("TARAL_UNIFORM") != nullptr;  // temporary A/B switch
-        const bool uniform = on && r1 - r0 > 1 && mx > kShort && mx <= 2 * mean + 8;
-        out.push_back(make_int4(r0, (r1 - r0) | (uniform ? kUniformRows : 0), int(ptr[r0]), int(ptr[r1])));
+        const bool uniform = r1 - r0 > 1 && mx > kShort && mx <= 2 * mean + 8;
+        out.push_back(make_int4(r0, (r1 - r0) | (uniform ? kUniformCandidate : 0), int(ptr[r0]), int(ptr[r1])));
     };
     int start = 0, cur_rows = 0;
     int64_t cur_nnz = 0;
@@ -108,13 +125,16 @@ struct Engine final : EngineBase {
     bool started = false;
 
     template <class U>
-    U* alloc(size_t count) {
+    U* alloc(size_t count) {  // stream-ordered, from the device's memory pool (see keep_pool_memory)
         void* p = nullptr;
-        cudaError_t e = cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(U));
+        const size_t bytes = std::max<size_t>(count, 1) * sizeof(U);
+        cudaError_t e = cudaMallocAsync(&p, bytes, st);
         if (e != cudaSuccess) throw CudaError{std::string("cudaMalloc: ") + cudaGetErrorString(e)};
         allocs.push_back(p);
+        alloc_bytes += bytes;
         return static_cast<U*>(p);
     }
+    size_t alloc_bytes = 0;
     T* upload(const double* v, size_t k) {
         std::vector<T> h(v, v + k);
         T* p = alloc<T>(k);
@@ -144,13 +164,11 @@ struct Engine final : EngineBase {
         return d;
     }
 
-    size_t free0 = 0;
     void begin(int m_, int n_, int freq, unsigned flags) {
         m = m_, n = n_, eval_freq = std::max(1, freq), use_graph = !(flags & TARAL_FLAG_NO_GRAPH);
-        size_t total;
-        CK(cudaMemGetInfo(&free0, &total));
         int dev;
         CK(cudaGetDevice(&dev));
+        keep_pool_memory(dev);
         cudaDeviceProp prop;
         CK(cudaGetDeviceProperties(&prop, dev));
         name = prop.name;
@@ -199,11 +217,12 @@ struct Engine final : EngineBase {
         double *va = nullptr, *vt = nullptr, *dr = nullptr, *dc = nullptr, *rs = nullptr, *cs = nullptr;
         struct Scratch {  // FP64 working values and factors, released when the set-up ends
             std::vector<void*> p;
-            ~Scratch() { for (void* q : p) cudaFree(q); }
-        } tmp;
+            cudaStream_t s;
+            ~Scratch() { for (void* q : p) cudaFreeAsync(q, s); }
+        } tmp{{}, st};
         auto scratch = [&](size_t count) {
             void* q = nullptr;
-            CK(cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(double)));
+            CK(cudaMallocAsync(&q, std::max<size_t>(count, 1) * sizeof(double), st));
             tmp.p.push_back(q);
             return static_cast<double*>(q);
         };
@@ -258,18 +277,73 @@ struct Engine final : EngineBase {
         CK(cudaMallocHost(&h_out, 32 * sizeof(double)));
         CK(cudaMallocHost(&h_flag, sizeof(int)));
         CK(cudaStreamSynchronize(st));
-        size_t free1, total;
-        CK(cudaMemGetInfo(&free1, &total));
-        mem_used = free0 - free1;
+        mem_used = alloc_bytes;
+        tune();
     }
     ~Engine() override {
         if (ev0) cudaEventDestroy(ev0), cudaEventDestroy(ev1);
         if (graph) cudaGraphExecDestroy(graph);
+        for (void* p : allocs) cudaFreeAsync(p, st);  // back to the pool: no device-wide synchronisation
         if (st) cudaStreamSynchronize(st);
-        for (void* p : allocs) cudaFree(p);
         if (h_out) cudaFreeHost(h_out);
         if (h_flag) cudaFreeHost(h_flag);
         if (st) cudaStreamDestroy(st);
+    }
+
+    // ------------------------------------------------------------------ autotuner
+    // Row-split policy per matrix (FP32 contexts, matrices of at least 2^20 nonzeros), timed on the matrix itself
+    // (CUDA-event time of 10 SpMV launches after 3 warm-ups): 0 the hybrid rule (thread per row up to 48 nonzeros,
+    // warp per longer row), 1 thread per row in the kUniformCandidate blocks, 2 the balanced segmented sums
+    // (kSegmented) in every block. A policy other than 0 is kept only if it is at least 5 % faster. FP64 contexts
+    // keep policy 0 (the parity pins' summation order); TARAL_TUNE=0 keeps it everywhere.
+    void tune() {
+        if (sizeof(T) != sizeof(float)) return;
+        if (const char* e = std::getenv("TARAL_TUNE"))
+            if (std::atoi(e) == 0) return;
+        int forced = -1;  // TARAL_ROWSPLIT=0|1|2: that policy for every matrix, untimed (tests, experiments)
+        if (const char* e = std::getenv("TARAL_ROWSPLIT")) forced = std::max(0, std::min(2, std::atoi(e)));
+        int which = 0;
+        for (DevMat* d : {&A, &AT}) {
+            const int slot = which++;
+            if (d->nblk == 0 || (forced < 0 && d->nnz < (int64_t(1) << 20))) continue;  // small: timings are noise
+            std::vector<int4> base(size_t(d->nblk));
+            CK(cudaMemcpyAsync(base.data(), d->blk, base.size() * sizeof(int4), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            std::vector<std::vector<int4>> cand(3, base);
+            bool uni = false;
+            for (int4& b : cand[1])
+                if (b.y & kUniformCandidate) b.y |= kUniformRows, uni = true;
+            for (int4& b : cand[2]) b.y |= kSegmented;
+            const T* xin = d == &A ? pv : pw;  // scratch vectors of the right length (power iteration)
+            T* yout = d == &A ? pw : pu;
+            auto time_list = [&](const std::vector<int4>& list) {
+                CK(cudaMemcpyAsync(d->blk, list.data(), list.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
+                for (int r = 0; r < 3; ++r) spmv(*d, xin, yout);
+                cudaEvent_t e0, e1;
+                CK(cudaEventCreate(&e0));
+                CK(cudaEventCreate(&e1));
+                CK(cudaEventRecord(e0, st));
+                for (int r = 0; r < 10; ++r) spmv(*d, xin, yout);
+                CK(cudaEventRecord(e1, st));
+                CK(cudaEventSynchronize(e1));
+                float ms = 0;
+                CK(cudaEventElapsedTime(&ms, e0, e1));
+                cudaEventDestroy(e0), cudaEventDestroy(e1);
+                launches -= 13;  // tuning launches are not part of the solve's count
+                return ms;
+            };
+            int best = 0;
+            if (forced >= 0) {
+                best = forced;
+            } else {
+                float t[3] = {time_list(cand[0]), uni ? time_list(cand[1]) : 1e30f, time_list(cand[2])};
+                for (int k = 1; k < 3; ++k)
+                    if (t[k] < 0.95f * t[0] && t[k] < t[best]) best = k;
+            }
+            tuned[slot] = best;
+            CK(cudaMemcpyAsync(d->blk, cand[best].data(), cand[best].size() * sizeof(int4), cudaMemcpyHostToDevice, st));
+            CK(cudaStreamSynchronize(st));
+        }
     }
 
     // ------------------------------------------------------------------ SpMV-shaped launches

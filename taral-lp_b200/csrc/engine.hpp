@@ -17,6 +17,7 @@ struct EngineBase {
     size_t mem_used = 0;
     int64_t launches = 0;
     int64_t nnz = 0;  // nonzeros of A
+    int tuned[2] = {0, 0};  // row-split policy chosen by the autotuner for A and A^T (1: thread per row)
     virtual ~EngineBase() = default;
     virtual double power_norm(int iters) = 0;
     virtual void set_steps(double tau, double sigma) = 0;
@@ -42,6 +43,7 @@ void engine_init(EngineBase& e, int precision, const taral_csr& A, const taral_c
                  const double* l, const double* u, const double* rl, const double* ru, const double* Dr,
                  const double* Dc, int m, int n, int eval_freq, unsigned flags);
 std::vector<int4> build_row_blocks(const int64_t* ptr, int rows);
+void keep_pool_memory(int dev);  // the device pool keeps freed memory for reuse by later contexts
 // Blocks of at most `tile` nonzeros and `rows_max` rows (a longer row is a block of its own).
 std::vector<int4> build_row_blocks(const int64_t* ptr, int rows, int tile, int rows_max);
 // Set-up from the column-wise model with the scaling done on the device, bit-identical to build_scaled(): P gets

@@ -126,22 +126,112 @@ struct EpiCol {
 // Row-block metadata, one int4 per block, built on the host (build_row_blocks): x = first row, y = number of rows,
 // z = first nonzero, w = end of the nonzeros. VEC: the val/idx base pointers are 16-byte aligned.
 constexpr int kShort = 48;                       // rows up to this length are summed by their own thread
-// Block flag (bit 16 of the metadata's row count): the block's rows have similar lengths (longest <= 2 x mean + 8),
-// so every row, however long, is summed by its own thread in entry order -- the warp path only pays off when a few
-// long rows would otherwise hold up a warp of short ones.
+// Block flags in the high bits of the metadata's row count (the row count itself is the low 16 bits):
+// kUniformRows -- every row of the block, however long, is summed by its own thread in entry order (the warp path
+//                 only pays off when a few long rows would otherwise hold up a warp of short ones). Set by the
+//                 autotuner (Engine::tune, Batch::tune) on kUniformCandidate blocks when that is measurably faster.
+// kUniformCandidate -- the block's rows have similar lengths (longest <= 2 x mean + 8) and some row exceeds kShort.
 constexpr int kUniformRows = 1 << 16;
+constexpr int kUniformCandidate = 1 << 17;
+// kSegmented -- balanced reduction: each thread sums kSeg consecutive products and rows crossing threads are joined
+//               by a segmented scan over the CTA (summation order fixed by the block's structure). Set by the
+//               autotuner on FP32 matrices when it is measurably faster.
+constexpr int kSegmented = 1 << 18;
+constexpr int kSeg = 8;
+static_assert(kSeg * kThreads >= kTile, "kSeg products per thread must cover a block");
 constexpr int kQuads = (kTile + 3 + 3) / 4 / kThreads;  // 16-byte quads per thread in the staging loop (2)
 static_assert(kQuads * 4 * kThreads >= kTile + 3, "a block's quads must fit the staging loop");
 __device__ __forceinline__ int pidx(int k) { return k + (k >> 5); }  // one pad slot per 32: no bank conflicts
+// 16-byte shared-memory accesses of 4 / 8 consecutive products (16-byte aligned addresses)
+__device__ __forceinline__ void store4(float* p, const float (&v)[4]) {
+    *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+__device__ __forceinline__ void store4(double* p, const double (&v)[4]) {
+    reinterpret_cast<double2*>(p)[0] = make_double2(v[0], v[1]);
+    reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
+}
+__device__ __forceinline__ void load8(const float* p, float (&v)[8]) {
+    const float4 a = reinterpret_cast<const float4*>(p)[0], b = reinterpret_cast<const float4*>(p)[1];
+    v[0] = a.x, v[1] = a.y, v[2] = a.z, v[3] = a.w, v[4] = b.x, v[5] = b.y, v[6] = b.z, v[7] = b.w;
+}
+__device__ __forceinline__ void load8(const double* p, double (&v)[8]) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const double2 a = reinterpret_cast<const double2*>(p)[i];
+        v[2 * i] = a.x, v[2 * i + 1] = a.y;
+    }
+}
 
 template <class P>
 struct RowSmem {
-    P prod[kTile + kTile / 32];
+    alignas(16) P prod[kTile + kTile / 32];  // hybrid: product k at pidx(k - p0); segmented: at k - (p0 & ~3)
     double rowsum[kRowsMax];
     int rptr[kRowsMax + 1];
     short longrow[kRowsMax];
     int nlong;
+    double segv[kThreads / 32];  // segmented scan: per-warp carry value and flag
+    int segf[kThreads / 32];
 };
+
+// Balanced row sums (kSegmented blocks) of the staged products sm.prod[pidx(0 .. len)], rows delimited by
+// sm.rptr[0 .. nrows]: thread t sums products [kSeg t, kSeg t + kSeg) in order. A row that starts and ends inside the
+// thread is written at once; the partial of a row that continues past the thread (its tail) is carried by a
+// segmented inclusive scan over the CTA (combine(a, b) = b started a row ? b : a + b), and the thread in which a
+// continued row ends adds the carried partial to its own head part. Ends with a barrier.
+template <class P>
+__device__ __forceinline__ void segmented_sums(RowSmem<P>& sm, int nrows) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int begin = sm.rptr[0], len = sm.rptr[nrows];  // entries [begin, len) of the unpadded product array
+    const int k0 = max(kSeg * tid, begin), k1 = min(kSeg * tid + kSeg, len);
+    double tail = 0, head = 0;
+    int head_row = -1, tail_starts = 1;  // tail_starts: the open segment (if any) began inside this thread
+    P pv[kSeg];
+    if (kSeg * tid < len) load8(&sm.prod[kSeg * tid], pv);  // this thread's 8 products, two 16-byte loads
+    if (k0 < k1) {
+        int lo = 0, hi = nrows - 1;  // the last row r with rptr[r] <= k0 (non-empty, since k0 < len)
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (sm.rptr[mid] <= k0) lo = mid;
+            else hi = mid - 1;
+        }
+        int r = lo;
+        bool cont = sm.rptr[r] < k0, first = true, open = false;
+        double acc = 0;
+        for (int k = k0; k < k1; ++k) {
+            acc += double(pv[k - kSeg * tid]);
+            open = true;
+            if (k + 1 == sm.rptr[r + 1]) {  // row r ends at k
+                if (first && cont) head = acc, head_row = r;
+                else sm.rowsum[r] = acc;
+                acc = 0, first = false, cont = false, open = false;
+                if (k + 1 < len)
+                    for (++r; sm.rptr[r + 1] == sm.rptr[r]; ++r) {}  // skip rows without entries
+            }
+        }
+        if (open) tail = acc, tail_starts = (first && cont) ? 0 : 1;  // a pure continuation carries on
+    }
+    // segmented inclusive scan of (tail, tail_starts) over the threads
+    double v = tail;
+    int f = tail_starts;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const double pv = __shfl_up_sync(0xffffffffu, v, off);
+        const int pf = __shfl_up_sync(0xffffffffu, f, off);
+        if (lane >= off) {
+            if (!f) v = pv + v;
+            f |= pf;
+        }
+    }
+    if (lane == 31) sm.segv[warp] = v, sm.segf[warp] = f;
+    __syncthreads();
+    double cv = 0;  // carry from the warps before this one
+    for (int w = 0; w < warp; ++w) cv = sm.segf[w] ? sm.segv[w] : cv + sm.segv[w];
+    const double incl = f ? v : cv + v;
+    double before = __shfl_up_sync(0xffffffffu, incl, 1);  // the scan value of the previous thread
+    if (lane == 0) before = cv;
+    if (head_row >= 0) sm.rowsum[head_row] = before + head;
+    __syncthreads();
+}
 
 // Sums of the block's rows into sm.rowsum[0, nrows) (a long row: sm.rowsum[0]). Ends with a barrier.
 //   1. stage: each thread issues all of its 16-byte val / idx loads (up to kQuads quads), then all of its gathers
@@ -184,9 +274,13 @@ __device__ __forceinline__ void block_sums(const int* __restrict__ ptr, const in
         return;
     }
 
-    // 1. stage products
-    for (int t = tid; t <= nrows; t += kThreads) sm.rptr[t] = ptr[r0 + t] - p0;
+    // 1. stage products (segmented blocks: unpadded, quad-aligned from a0 = p0 & ~3, for 16-byte accesses)
+    const bool seg = (meta.y & kSegmented) != 0;
+    const int base = seg ? (p0 & ~3) : p0;
+    for (int t = tid; t <= nrows; t += kThreads) sm.rptr[t] = ptr[r0 + t] - base;
     if (tid == 0) sm.nlong = 0;
+    if (seg)  // rows without entries stay zero; every other row is written once, after the barrier
+        for (int t = tid; t < nrows; t += kThreads) sm.rowsum[t] = 0;
     if (VEC) {
         const int a0 = p0 & ~3;
         T v[kQuads][4];
@@ -210,18 +304,36 @@ __device__ __forceinline__ void block_sums(const int* __restrict__ ptr, const in
         for (int i = 0; i < kQuads; ++i)
 #pragma unroll
             for (int e = 0; e < 4; ++e) g[i][e] = c[i][e] >= 0 ? gather(xin + c[i][e]) : X(0);
+        if (seg) {
 #pragma unroll
-        for (int i = 0; i < kQuads; ++i) {
-            const int q = a0 + 4 * (tid + i * kThreads);
+            for (int i = 0; i < kQuads; ++i) {
+                const int q = a0 + 4 * (tid + i * kThreads);
+                if (q < p1) {
+                    P pq[4];
 #pragma unroll
-            for (int e = 0; e < 4; ++e)
-                if (c[i][e] >= 0) sm.prod[pidx(q + e - p0)] = P(v[i][e]) * P(g[i][e]);
+                    for (int e = 0; e < 4; ++e) pq[e] = c[i][e] >= 0 ? P(P(v[i][e]) * P(g[i][e])) : P(0);
+                    store4(&sm.prod[q - a0], pq);
+                }
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < kQuads; ++i) {
+                const int q = a0 + 4 * (tid + i * kThreads);
+#pragma unroll
+                for (int e = 0; e < 4; ++e)
+                    if (c[i][e] >= 0) sm.prod[pidx(q + e - p0)] = P(v[i][e]) * P(g[i][e]);
+            }
         }
     } else {
-        for (int k = p0 + tid; k < p1; k += kThreads) sm.prod[pidx(k - p0)] = P(__ldg(val + k)) * P(__ldg(xin + __ldg(idx + k)));
+        for (int k = p0 + tid; k < p1; k += kThreads)
+            sm.prod[seg ? k - base : pidx(k - p0)] = P(__ldg(val + k)) * P(__ldg(xin + __ldg(idx + k)));
     }
     __syncthreads();
 
+    if (seg) {
+        segmented_sums(sm, nrows);
+        return;
+    }
     // 2. reduce: short rows (every row of a uniform block) by their own thread, long rows by a warp each
     const int thread_max = (meta.y & kUniformRows) ? kTile : kShort;
     if (tid < nrows) {
