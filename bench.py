@@ -50,6 +50,16 @@ METRIC = "time-to-1e-6 rel KKT per LP"
 REF_SAMPLE_ITERS = 256
 
 
+def dist_max(v, dist, device="cuda"):
+    """The maximum over ranks of a per-rank time (whole-job time of the replicas); v itself with one rank."""
+    if not dist:
+        return v
+    import torch
+    t = torch.tensor([float(v)], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return t.item()
+
+
 def peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -239,10 +249,7 @@ def our_arm(args, rank, world, dist):
         flush_l2(torch, flush)
     barrier()
     clk = clocks.stop()
-    t = torch.tensor([dev_s], dtype=torch.float64, device="cuda")
-    if dist:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    value = t.item() / (world * args.steps)
+    value = dist_max(dev_s, dist) / (world * args.steps)  # LPs of all replicas / the slowest rank's time
 
     # e2e through the public API from host arrays (scaling, upload, solve, download, check every step), after one
     # untimed call (the first call in a process also loads the library's kernels)
@@ -256,10 +263,7 @@ def our_arm(args, rank, world, dist):
         e2e_steps.append(time.perf_counter() - ts)
         e2e_out.append(r)
     torch.cuda.synchronize()
-    e2e_s = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device="cuda")
-    if dist:
-        torch.distributed.all_reduce(e2e_s, op=torch.distributed.ReduceOp.MAX)
-    e2e_value = e2e_s.item() / (world * args.steps)
+    e2e_value = dist_max(time.perf_counter() - t0, dist) / (world * args.steps)
     nnz = e2e_out[0]["nnz"]
     m, n = lp.m, lp.n
     # uploaded per solve: A and A^T unscaled (int32 ptr, int32 idx, f64 val: scaled and narrowed on the device),
