@@ -10,11 +10,15 @@ Needs the reference checkout (REF, default /root/reference) and the reference bi
 * reference_runs.json    reference `pdhg --device cpu --threads 1` (FP64) reports on generated models
 * reference_vectors.npz  the .sol / .dual vectors of those runs
 * reference_optima.json  the reference IPM optimum (`taral --method ipm`) of the planted 2000 x 5000 model
+* reference_vector_check.json (with --vector-check) the reference's independent answer check
+                         (gpu/vector_check.check_files) on the .sol / .dual of the runs in reference_runs.json
+* reference_refinery_T4.json (with --refinery, ~2 minutes of CPU) the reference dual simplex optimum of one
+                         4-period scenario of the refinery family (RefineryBase(48, seed=7), perturbations(2, seed=3)[0])
 * reference_bench_lp.json (with --bench-lp, minutes of CPU) the reference `pdhg --device cpu` FP64 report on the
                          benchmark LP (planted, Zipf rows, 200,000 x 500,000, seed 0) solved to 1e-6: the FP64
                          iteration count the benchmark's CPU baselines are projected to
 
-Run from the repository root: python tests/golden/make_golden.py [--bench-lp]
+Run from the repository root: python tests/golden/make_golden.py [--bench-lp | --refinery | --vector-check]
 """
 import csv
 import hashlib
@@ -138,8 +142,48 @@ def bench_lp():
     print("wrote reference_bench_lp.json:", out["status"], out["iterations"])
 
 
+def vector_check():
+    sys.path.insert(0, str(REF / "gpu"))
+    import vector_check as vc  # the reference's checker (needs REF/benchmarks/orig_check.py)
+    vecs = np.load(OUT / "reference_vectors.npz")
+    out = {}
+    with tempfile.TemporaryDirectory() as td:
+        td = Path(td)
+        for name, make, _ in RUNS:
+            lp = make()
+            rn, cn = lp._names()
+            f, sol, dual = td / "m.mps", td / "m.sol", td / "m.dual"
+            lp.write_mps(f)
+            sol.write_text("".join(f"{c} {v:.17g}\n" for c, v in zip(cn, vecs[name + "/x"])))
+            dual.write_text("".join(f"{r} {v:.17g}\n" for r, v in zip(rn, vecs[name + "/y"])))
+            out[name] = {"model_sha256": lp.digest(), **vc.check_files(str(f), str(sol), str(dual))}
+    (OUT / "reference_vector_check.json").write_text(json.dumps(out, indent=1) + "\n")
+    print("wrote reference_vector_check.json:", len(out), "runs")
+
+
+def refinery():
+    if not TARAL.exists():
+        sys.exit("build the reference first: make -C oracle ref")
+    lp = lpgen.RefineryBase(48, seed=7).instance(4, lpgen.perturbations(2, seed=3)[0])
+    with tempfile.TemporaryDirectory() as td:
+        f, j = Path(td) / "r.mps", Path(td) / "r.json"
+        lp.write_mps(f)
+        subprocess.run([str(TARAL), str(f), "--method", "dual", "--time-limit", "600", "--json", str(j)], check=True,
+                       stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        rep = json.loads(j.read_text())
+    out = {"scenario": "RefineryBase(48, seed=7).instance(4, perturbations(2, seed=3)[0])", "method": "dual",
+           "model_sha256": lp.digest(), "rows": lp.m, "cols": lp.n, "nnz": lp.nnz,
+           **{k: rep.get(k) for k in ("status", "objective", "dual_objective", "primal_res", "dual_res", "gap")}}
+    (OUT / "reference_refinery_T4.json").write_text(json.dumps(out, indent=1) + "\n")
+    print("wrote reference_refinery_T4.json:", out["status"], out["objective"])
+
+
 if __name__ == "__main__":
     if "--bench-lp" in sys.argv:
         bench_lp()
+    elif "--refinery" in sys.argv:
+        refinery()
+    elif "--vector-check" in sys.argv:
+        vector_check()
     else:
         main()
