@@ -354,10 +354,15 @@ def family_arm(args):
     gen_s = time.perf_counter() - t0
     t0 = time.perf_counter()
     b = pdhg.Batch(lps, tol=tol, precision=pdhg.FP32, time_limit=3000)
-    res, _, _ = b.solve(want_points=False)
+    res, bx, by = b.solve()
     batch_s = time.perf_counter() - t0
     info = b.info()
     b.close()
+    # independent FP64 check of every answer on its original model, on the device (not part of the timed solve)
+    t0 = time.perf_counter()
+    chk = pdhg.check_models(lps, bx, by)
+    check_s = time.perf_counter() - t0
+    del bx, by
     order = np.argsort(periods, kind="stable")
     pick = order[np.linspace(0, len(order) - 1, min(args.sample, len(order))).round().astype(int)]
     plain_t, plain_T, obj_diff = [], [], []
@@ -391,6 +396,13 @@ def family_arm(args):
                                       "sample_periods": plain_T, "sample_s": plain_t,
                                       "fit_s_per_period": float(slope), "fit_intercept_s": float(icpt)},
             "speedup_per_lp": plain_per_lp / (batch_s / k),
+            "independent_check": {"seconds": check_s,
+                                  "max_row_violation_rel": max(c["row_violation_rel"] for c in chk),
+                                  "max_bound_violation": max(c["bound_violation"] for c in chk),
+                                  "max_dual_gap_rel": max(abs(c["dual_gap_rel"]) for c in chk if c["dual_gap_rel"] is not None),
+                                  "strict_dual_bounds": sum(c["dual_bound"] is not None for c in chk),
+                                  "max_objective_diff_vs_solver": max(abs(c["objective"] - r["objective"]) /
+                                                                      max(1.0, abs(r["objective"])) for c, r in zip(chk, res))},
             "objective_max_rel_diff_batched_vs_plain": float(max(obj_diff)), "generate_s": gen_s}
     print(json.dumps(line))
 

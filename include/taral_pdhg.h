@@ -210,7 +210,7 @@ int taral_spmv_plan_blocks(const taral_spmv_plan* plan);
 void taral_spmv_plan_destroy(taral_spmv_plan* plan);
 
 /* ------------------------------------------------------------------------------------------------------------
- * 5. Batched solve: many LPs of one scenario family in one context (SURVEY: the batched scenario family). No
+ * 5. Batched solve: many LPs of one scenario family in one context (the batched scenario family). No
  *    counterpart in the reference, which solves one model per process (gpu/pdhg.cu:937-992); each instance
  *    follows the reference driver's rules (gpu/pdhg.cu:761-849) with its own step sizes, primal weight,
  *    restarts and stopping, evaluated on the device so a block of eval_freq iterations for the whole batch is
@@ -285,6 +285,31 @@ int taral_kkt_eval_noalloc(int m, int n, int dtype, double f, const void* Ax, co
                            const void* ru, const void* Dr, const void* zlast, const void* x, const void* ATz,
                            const void* c, const void* l, const void* u, const void* Dc, const void* xlast,
                            double* out10, void* stream);
+
+/* ------------------------------------------------------------------------------------------------------------
+ * 8. Independent check of answers on the original models, on the device (FP64), for one model or a whole batch:
+ *    the reference checker's semantics -- benchmarks/orig_check.py:63-88 (objective incl. the objective row's
+ *    constant, largest row violation relative to 1 + |b|, largest bound violation) and gpu/vector_check.py:46-74
+ *    (weak-duality bound LB(y) for y and -y, d = c - A'y; a term whose minimising bound is infinite, |v| >= 1e20,
+ *    is dropped and recorded as dual infeasibility; the sign with the smaller one is kept). Shares no code with the
+ *    solver: the models are uploaded unscaled in FP64.
+ * ------------------------------------------------------------------------------------------------------------ */
+typedef struct taral_check {
+    double objective;         /* c'x + obj_const */
+    double row_violation_rel; /* max_i max(lo_i - a_i x, a_i x - up_i, 0) / (1 + |b_i|) */
+    double bound_violation;   /* max_j max(l_j - x_j, x_j - u_j, 0) */
+    double dual_bound;        /* strict weak-duality bound; NaN when a term was dropped or the dual is not checked */
+    double dual_obj_loose;    /* LB with dropped terms left out (not a rigorous bound); NaN when not checked */
+    double dual_infeas_rel;   /* the largest dropped term, relative; NaN when not checked */
+    double dual_gap_rel;      /* (objective - dual_obj_loose) / max(1, |objective|); NaN when not checked */
+    int dual_sign;            /* +1 or -1: the sign of y used; 0: not checked (no y, or a maximisation model) */
+    int pad;
+} taral_check;
+/* x[i] (n_i, original space) and optional y[i] (m_i, row multipliers; y or y itself NULL: primal side only) of
+ * model i. rhs: NULL, or per model NULL or the rows' right-hand sides b (the MPS RHS values; default: b = lo where
+ * lo is finite, else up). out[i]: model i's check. */
+int taral_check_models(const taral_model* models, int count, const double* const* rhs, const double* const* x,
+                       const double* const* y, taral_check* out);
 
 #ifdef __cplusplus
 }

@@ -22,7 +22,7 @@ PROBE = PKG / "bin" / "gather_probe"
 NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-O3", "-I", str(ROOT / "include")]
-SOURCES = ["engine.cu", "batch.cu", "noalloc.cu", "mlp.cu", "mlp_tc.cu", "scaling.cpp", "mps.cpp", "solve.cpp"]
+SOURCES = ["engine.cu", "batch.cu", "noalloc.cu", "mlp.cu", "mlp_tc.cu", "verify.cu", "scaling.cpp", "mps.cpp", "solve.cpp"]
 
 
 def _headers():

@@ -634,7 +634,7 @@ struct Batch final : BatchBase {
             sh.S.m = mk.m, sh.S.n = mk.n, sh.nnz = int64_t(sh.S.A.idx.size());
         });
         // 3. concatenated matrices (int32 offsets), uploaded unscaled and scaled on the device (scaling.cuh:
-        //    bit-identical to scale_matrix), values narrowed to T in place
+        //    bit-identical to the reference's host scaling), values narrowed to T in place
         std::vector<int> hAptr, hTptr;
         int64_t nzb = 0;
         int drn = 0, dcn = 0;

@@ -46,7 +46,7 @@ std::vector<int4> build_row_blocks(const int64_t* ptr, int rows);
 void keep_pool_memory(int dev);  // the device pool keeps freed memory for reuse by later contexts
 // Blocks of at most `tile` nonzeros and `rows_max` rows (a longer row is a block of its own).
 std::vector<int4> build_row_blocks(const int64_t* ptr, int rows, int tile, int rows_max);
-// Set-up from the column-wise model with the scaling done on the device, bit-identical to build_scaled(): P gets
+// Set-up from the column-wise model with the scaling done on the device, bit-identical to the reference's: P gets
 // Dr, Dc, the scaled vectors and the norms (its matrices stay empty); host_s: seconds of host work.
 struct Scaled;
 void engine_init_model(EngineBase& e, int precision, const taral_model& md, double sign, Scaled& P, int eval_freq,

@@ -45,8 +45,7 @@ struct Csr {
     std::vector<double> val;
     taral_csr view(int cols) const { return {rows, cols, int64_t(val.size()), ptr.data(), idx.data(), val.data()}; }
 };
-Csr transpose(const Csr& a, int cols);  // gpu/pdhg.cu:55-70
-// transpose() of the CSR given by (ptr, idx, val) with the scatter on `threads` threads; identical output.
+// Transpose of the CSR given by (ptr, idx, val) (gpu/pdhg.cu:55-70), the scatter on `threads` threads.
 Csr transpose_par(const int64_t* ptr, const int32_t* idx, const double* val, int rows, int cols, int threads);
 int host_threads();
 
@@ -58,14 +57,12 @@ struct Scaled {
     double bnorm = 0, cnorm = 0;  // original-space norms of the stopping test
     bool a_original = false;      // A holds the UNSCALED row-wise matrix (device-side set-up), used by finish_point
 };
-Scaled build_scaled(const taral_model& md, double sign);  // gpu/pdhg.cu:80-133
-// The two halves of build_scaled: the matrix part (A_s, A_s^T, Dr, Dc: depends on A only) and the vector part
-// (c, l, u, rl, ru and the original-space norms, given Dr and Dc). Instances that share A share the first.
-void scale_matrix(const taral_model& md, Scaled& P);
+// The vector part of the scaled problem (c, l, u, rl, ru and the original-space norms) given Dr and Dc
+// (gpu/pdhg.cu:113-133).
 void scale_vectors(const taral_model& md, double sign, const std::vector<double>& Dr, const std::vector<double>& Dc,
                    Scaled& P);
 // The unscaled A (the transpose of the column-wise model with explicit zeros dropped) and A^T (the transpose of A):
-// the structure and entry order scale_matrix() works on (gpu/pdhg.cu:80-90, 131), before any scaling.
+// the structure and entry order the reference's scaling works on (gpu/pdhg.cu:80-90, 131), before any scaling.
 void model_matrices(const taral_model& md, Csr& A, Csr& AT, int threads = 0);  // threads <= 0: host_threads()
 
 struct Options {  // gpu/pdhg.cu:744-750

@@ -1,5 +1,6 @@
-// Host preprocessing: CSR transpose and Ruiz / Pock-Chambolle scaling (gpu/pdhg.cu:55-133 semantics).
-// FP64, single pass order identical to the reference so the scaled matrix is bit-identical to it.
+// Host preprocessing: the CSR transposes of the model (gpu/pdhg.cu:55-70 semantics), the scaled vectors and norms
+// (gpu/pdhg.cu:113-133) given the scaling factors computed on the device (scaling.cuh), and the original-space check
+// of an answer (gpu/pdhg.cu:866-876).
 #include <algorithm>
 #include <cmath>
 #include <thread>
@@ -8,26 +9,9 @@
 
 namespace taral {
 
-Csr transpose(const Csr& a, int cols) {  // counting sort; rows of the output ascending (gpu/pdhg.cu:55-70)
-    Csr t;
-    t.rows = cols;
-    t.ptr.assign(size_t(cols) + 1, 0);
-    for (int32_t k : a.idx) t.ptr[size_t(k) + 1]++;
-    for (int j = 0; j < cols; ++j) t.ptr[j + 1] += t.ptr[j];
-    t.idx.resize(a.idx.size());
-    t.val.resize(a.val.size());
-    std::vector<int64_t> pos(t.ptr.begin(), t.ptr.end() - 1);
-    for (int i = 0; i < a.rows; ++i)
-        for (int64_t k = a.ptr[i]; k < a.ptr[i + 1]; ++k) {
-            int64_t p = pos[a.idx[k]]++;
-            t.idx[p] = i, t.val[p] = a.val[k];
-        }
-    return t;
-}
-
-// The same counting sort with the scatter split over threads by ranges of output rows: every thread reads the
-// whole input in order and writes only its own rows, so each output row is filled in the sequential order and the
-// result is identical to transpose().
+// CSR transpose by counting sort (gpu/pdhg.cu:55-70 semantics: rows of the output ascending), the scatter split
+// over threads by ranges of output rows: every thread reads the whole input in order and writes only its own rows,
+// so each output row is filled in the sequential order and the result does not depend on the thread count.
 Csr transpose_par(const int64_t* ptr, const int32_t* idx, const double* val, int rows, int cols, int threads) {
     Csr t;
     t.rows = cols;
@@ -101,54 +85,6 @@ void model_matrices(const taral_model& md, Csr& A, Csr& AT, int threads) {
     }
 }
 
-void scale_matrix(const taral_model& md, Scaled& P) {
-    P.n = md.n, P.m = md.m;
-    Csr T;  // A^T from the column-wise model, zero entries dropped
-    T.rows = P.n;
-    T.ptr.assign(size_t(P.n) + 1, 0);
-    T.idx.reserve(size_t(md.col_ptr[P.n] - md.col_ptr[0]));
-    T.val.reserve(size_t(md.col_ptr[P.n] - md.col_ptr[0]));
-    for (int j = 0; j < P.n; ++j) {
-        for (int64_t k = md.col_ptr[j]; k < md.col_ptr[j + 1]; ++k)
-            if (md.val[k] != 0) T.idx.push_back(md.row_idx[k]), T.val.push_back(md.val[k]);
-        T.ptr[j + 1] = int64_t(T.idx.size());
-    }
-    P.A = transpose(T, P.m);
-    T = Csr();
-    Csr& A = P.A;
-    P.Dr.assign(size_t(P.m), 1), P.Dc.assign(size_t(P.n), 1);
-    std::vector<double> rs(size_t(P.m)), cs(size_t(P.n));
-    auto apply = [&] {  // divide by sqrt of the row and column measures, fold the factors into Dr, Dc
-        for (double& v : rs) v = v > 0 ? std::sqrt(v) : 1;
-        for (double& v : cs) v = v > 0 ? std::sqrt(v) : 1;
-        for (int i = 0; i < P.m; ++i) {
-            const double ri = rs[i];
-            for (int64_t k = A.ptr[i]; k < A.ptr[i + 1]; ++k) A.val[k] /= ri * cs[A.idx[k]];
-        }
-        for (int i = 0; i < P.m; ++i) P.Dr[i] /= rs[i];
-        for (int j = 0; j < P.n; ++j) P.Dc[j] /= cs[j];
-    };
-    for (int pass = 0; pass < 10; ++pass) {  // Ruiz equilibration, inf-norm
-        std::fill(rs.begin(), rs.end(), 0.0), std::fill(cs.begin(), cs.end(), 0.0);
-        for (int i = 0; i < P.m; ++i) {
-            double ri = 0;
-            for (int64_t k = A.ptr[i]; k < A.ptr[i + 1]; ++k) {
-                double a = std::fabs(A.val[k]);
-                ri = std::max(ri, a);
-                double& cj = cs[A.idx[k]];
-                cj = std::max(cj, a);
-            }
-            rs[i] = ri;
-        }
-        apply();
-    }
-    std::fill(rs.begin(), rs.end(), 0.0), std::fill(cs.begin(), cs.end(), 0.0);  // Pock-Chambolle, alpha = 1
-    for (int i = 0; i < P.m; ++i)
-        for (int64_t k = A.ptr[i]; k < A.ptr[i + 1]; ++k) rs[i] += std::fabs(A.val[k]), cs[A.idx[k]] += std::fabs(A.val[k]);
-    apply();
-    P.AT = transpose(A, P.n);
-}
-
 void scale_vectors(const taral_model& md, double sign, const std::vector<double>& Dr, const std::vector<double>& Dc,
                    Scaled& P) {
     P.m = md.m, P.n = md.n;
@@ -169,13 +105,6 @@ void scale_vectors(const taral_model& md, double sign, const std::vector<double>
         P.rl[i] = lo * Dr[i], P.ru[i] = up * Dr[i];
     }
     P.bnorm = std::sqrt(P.bnorm), P.cnorm = std::sqrt(P.cnorm);
-}
-
-Scaled build_scaled(const taral_model& md, double sign) {
-    Scaled P;
-    scale_matrix(md, P);
-    scale_vectors(md, sign, P.Dr, P.Dc, P);
-    return P;
 }
 
 Finished finish_point(const taral_model& md, const Scaled& P, const Outcome& r) {

@@ -1,6 +1,6 @@
 // Ruiz (10 passes, inf-norm) and Pock-Chambolle (alpha = 1) scaling on the device (gpu/pdhg.cu:92-130), applied to
 // the unscaled A and A^T together. Every value is produced by the same FP64 operations on the same operands as the
-// host scale_matrix(), so the scaled matrices, Dr and Dc are bit-identical to it:
+// reference's host scaling (gpu/pdhg.cu:92-130), so the scaled matrices, Dr and Dc are bit-identical to it:
 //   * row / column maxima: a max is independent of the visiting order (the comparison keeps the current value when
 //     the new one is not larger, as std::max does, so a NaN entry is never taken);
 //   * square roots and divisions are IEEE round-to-nearest in CUDA double precision, and v / (r_i * c_j) has no

@@ -65,6 +65,12 @@ class OutcomeT(C.Structure):
                 ("nnz", C.c_int64), ("device_s", C.c_double)]
 
 
+class CheckT(C.Structure):
+    _fields_ = [(k, C.c_double) for k in ("objective", "row_violation_rel", "bound_violation", "dual_bound",
+                                          "dual_obj_loose", "dual_infeas_rel", "dual_gap_rel")] + \
+               [("dual_sign", C.c_int), ("pad", C.c_int)]
+
+
 # Every symbol the header declares, with its ctypes signature: (restype, argtypes).
 SIGNATURES = {
     "pdhg_create": (C.c_int, [C.POINTER(CsrT), C.POINTER(CsrT)] + [_dp] * 7 +
@@ -103,6 +109,7 @@ SIGNATURES = {
                                    C.POINTER(C.c_int64)]),
     "taral_batch_last_error": (C.c_char_p, [C.c_void_p]),
     "taral_batch_destroy": (None, [C.c_void_p]),
+    "taral_check_models": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "taral_kkt_eval_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double] + [C.c_void_p] * 13 +
                                [C.c_void_p, C.c_void_p]),
     "taral_mlp_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
@@ -325,6 +332,46 @@ def solve(lp, tol=1e-4, time_limit=3600.0, max_iter=2_000_000_000, eval_freq=64,
     out = {k: getattr(r, k) for k, _ in OutcomeT._fields_}
     out["status"] = STATUS[r.status]
     return out, x[:lp.n], y[:lp.m]
+
+
+# ------------------------------------------------------------------------------------------------ check
+def rhs_of(lp):
+    """The rows' MPS right-hand sides b when the model knows its row types (up for L rows, lo otherwise, as the MPS
+    writer puts them), else None (the library's default: b = lo where lo is finite, else up)."""
+    types = getattr(lp, "row_types", None)
+    if types is None:
+        return None
+    return np.where(np.asarray(types) == "L", np.asarray(lp.row_up, float), np.asarray(lp.row_lo, float))
+
+
+def check_models(lps, xs, ys=None, rhs=None):
+    """Independent FP64 check of answers on the original models, on the device (taral_check_models): a list of dicts
+    with objective, row_violation_rel, bound_violation and the weak-duality fields (None where not checked)."""
+    k = len(lps)
+    models = [_Model(lp) for lp in lps]
+    arr = (ModelT * k)(*[m.s for m in models])
+    xa = [_f64(x) for x in xs]
+    ya = None if ys is None else [None if y is None else _f64(y) for y in ys]
+    ra = [rhs_of(lp) for lp in lps] if rhs is None else rhs
+    ra = [None if r is None else _f64(r) for r in ra]
+
+    def table(vs):
+        if vs is None:
+            return None, None
+        t = (_dp * k)(*[None if v is None else _p(v) for v in vs])
+        return t, C.cast(t, C.c_void_p)
+    tx, ty, tr = table(xa), table(ya), table(ra)
+    out = (CheckT * k)()
+    _check(lib().taral_check_models(C.cast(arr, C.c_void_p), k, tr[1], tx[1], ty[1], C.cast(out, C.c_void_p)))
+    res = []
+    for o in out:
+        d = {f: getattr(o, f) for f, _ in CheckT._fields_ if f != "pad"}
+        for f in ("dual_bound", "dual_obj_loose", "dual_infeas_rel", "dual_gap_rel"):
+            if np.isnan(d[f]):
+                d[f] = None
+        d["dual_sign"] = None if d["dual_sign"] == 0 else float(d["dual_sign"])
+        res.append(d)
+    return res
 
 
 # ------------------------------------------------------------------------------------------------ batch
