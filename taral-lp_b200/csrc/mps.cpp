@@ -14,6 +14,7 @@
 #include <sstream>
 #include <charconv>
 #include <string_view>
+#include <thread>
 #include <unordered_map>
 #include <unordered_set>
 
@@ -94,30 +95,38 @@ struct Entry {
     double v;
 };
 
-// Name -> index for the ROWS and COLUMNS names: open addressing with linear probing over views into the file
-// buffer (the buffer outlives the table), 64-bit FNV-1a hashes kept per slot, grown at half load.
+// Name -> index for the ROWS and COLUMNS names: open addressing with linear probing, grown at half load. A slot
+// is 8 bytes (the upper half of a 64-bit FNV-1a hash and the index), so a probe costs one cache line; a tag match
+// is confirmed against the name of that index, a view into the file buffer (the buffer outlives the table).
 class NameTable {
   public:
     explicit NameTable(size_t expect) { rehash(std::max<size_t>(64, next_pow2(2 * expect))); }
     const int* find(std::string_view k) const {
         const uint64_t h = hash(k);
+        const uint32_t tag = uint32_t(h >> 32);
         for (size_t i = h & mask_;; i = (i + 1) & mask_) {
-            if (idx_[i] < 0) return nullptr;
-            if (hash_[i] == h && key_[i] == k) return &idx_[i];
+            const Slot& s = slot_[i];
+            if (s.idx < 0) return nullptr;
+            if (s.tag == tag && name_[size_t(s.idx)] == k) return &s.idx;
         }
     }
     bool count(std::string_view k) const { return find(k) != nullptr; }
-    void insert(std::string_view k, int v) {  // k must not be present
-        if (2 * (n_ + 1) > key_.size()) rehash(2 * key_.size());
-        place(k, hash(k), v);
-        ++n_;
+    int add(std::string_view k) {  // k must not be present; indices are 0, 1, 2, ... in insertion order
+        if (2 * (name_.size() + 1) > slot_.size()) rehash(2 * slot_.size());
+        const int v = int(name_.size());
+        name_.push_back(k);
+        place(hash(k), v);
+        return v;
     }
 
   private:
-    std::vector<std::string_view> key_;
-    std::vector<uint64_t> hash_;
-    std::vector<int> idx_;
-    size_t mask_ = 0, n_ = 0;
+    struct Slot {
+        uint32_t tag;
+        int idx;
+    };
+    std::vector<Slot> slot_;
+    std::vector<std::string_view> name_;
+    size_t mask_ = 0;
     static size_t next_pow2(size_t x) {
         size_t p = 1;
         while (p < x) p <<= 1;
@@ -128,21 +137,84 @@ class NameTable {
         for (unsigned char c : k) h = (h ^ c) * 1099511628211ull;
         return h ^ (h >> 29);
     }
-    void place(std::string_view k, uint64_t h, int v) {
+    void place(uint64_t h, int v) {
         size_t i = h & mask_;
-        while (idx_[i] >= 0) i = (i + 1) & mask_;
-        key_[i] = k, hash_[i] = h, idx_[i] = v;
+        while (slot_[i].idx >= 0) i = (i + 1) & mask_;
+        slot_[i] = {uint32_t(h >> 32), v};
     }
     void rehash(size_t size) {
-        std::vector<std::string_view> k(std::move(key_));
-        std::vector<uint64_t> h(std::move(hash_));
-        std::vector<int> v(std::move(idx_));
-        key_.assign(size, std::string_view()), hash_.assign(size, 0), idx_.assign(size, -1);
+        slot_.assign(size, Slot{0, -1});
         mask_ = size - 1;
-        for (size_t i = 0; i < v.size(); ++i)
-            if (v[i] >= 0) place(k[i], h[i], v[i]);
+        for (size_t v = 0; v < name_.size(); ++v) place(hash(name_[v]), int(v));
     }
 };
+
+// One entry of the COLUMNS section, tokenised: an entry (col, row as row_of gives it, value) or a MARKER line
+// (kind 1: INTORG, 2: INTEND).
+struct ColRec {
+    std::string_view col;
+    int row;
+    int kind;
+    double v;
+};
+
+bool is_header(std::string_view line) {  // a section header: not blank, not a comment, not indented
+    return line.find_first_not_of(" \t") != std::string_view::npos && line[0] != ' ' && line[0] != '\t' &&
+           line[0] != '*';
+}
+
+// Tokenise the free-format COLUMNS lines in [b, e) of buf on `threads` threads (line-aligned chunks, one record
+// list each; read in chunk order they are in file order). Returns false if any line is malformed: the caller then
+// parses sequentially, which reports the same first error as always.
+template <class RowOf>
+bool tokenize_columns(const std::string& buf, size_t b, size_t e, int threads, const RowOf& row_of,
+                      std::vector<std::vector<ColRec>>& parts) {
+    std::vector<size_t> cut{b};
+    for (int q = 1; q < threads; ++q) {
+        size_t p = b + (e - b) * size_t(q) / size_t(threads);
+        p = std::max(p, cut.back());
+        const size_t nl = buf.find('\n', p);
+        cut.push_back(nl == std::string::npos || nl >= e ? e : nl + 1);
+    }
+    cut.push_back(e);
+    const size_t nparts = static_cast<size_t>(threads);
+    parts.assign(nparts, std::vector<ColRec>());
+    std::vector<char> bad(nparts, 0);
+    auto work = [&](int q) {
+        std::vector<std::string_view> t;
+        std::vector<ColRec>& r = parts[size_t(q)];
+        r.reserve((cut[size_t(q) + 1] - cut[size_t(q)]) / 16 + 16);  // an entry takes at least 16 bytes of text
+        try {
+            for (size_t pos = cut[size_t(q)]; pos < cut[size_t(q) + 1];) {
+                size_t nl = buf.find('\n', pos);
+                if (nl == std::string::npos || nl > cut[size_t(q) + 1]) nl = cut[size_t(q) + 1];
+                std::string_view line(buf.data() + pos, nl - pos);
+                pos = nl + 1;
+                if (!line.empty() && line.back() == '\r') line.remove_suffix(1);
+                if (line.find_first_not_of(" \t") == std::string_view::npos || line[0] == '*') continue;
+                split(line, "COLUMNS", false, t);
+                if (t.size() >= 2 && t[1] == "'MARKER'") {
+                    bool st = false, en = false;
+                    for (std::string_view w : t) st |= w == "'INTORG'", en |= w == "'INTEND'";
+                    if (st == en) throw ParseError("bad MARKER line");
+                    r.push_back({std::string_view(), 0, st ? 1 : 2, 0.0});
+                    continue;
+                }
+                if (t.size() != 3 && t.size() != 5) throw ParseError("bad COLUMNS line");
+                for (size_t k = 1; k + 1 < t.size(); k += 2) r.push_back({t[0], row_of(t[k]), 0, parse_number(t[k + 1])});
+            }
+        } catch (const ParseError&) {
+            bad[size_t(q)] = 1;
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int q = 1; q < threads; ++q) pool.emplace_back(work, q);
+    work(0);
+    for (auto& th : pool) th.join();
+    for (char x : bad)
+        if (x) return false;
+    return true;
+}
 
 std::string read_file(const std::string& path) {
     std::ifstream in(path, std::ios::binary);
@@ -176,7 +248,17 @@ Model parse(const std::string& path, bool fixed) {
 
     auto close_column = [&] {  // sorted by row, duplicates summed in file order, zero sums dropped
         if (cur < 0) return;
-        std::stable_sort(pending.begin(), pending.end(), [](const Entry& a, const Entry& b) { return a.row < b.row; });
+        if (pending.size() <= 32) {  // stable insertion sort: no buffer to allocate per column
+            for (size_t k = 1; k < pending.size(); ++k) {
+                const Entry e = pending[k];
+                size_t w = k;
+                for (; w > 0 && pending[w - 1].row > e.row; --w) pending[w] = pending[w - 1];
+                pending[w] = e;
+            }
+        } else {
+            std::stable_sort(pending.begin(), pending.end(),
+                             [](const Entry& a, const Entry& b) { return a.row < b.row; });
+        }
         size_t start = md.row_idx.size();
         for (const Entry& e : pending) {
             if (md.row_idx.size() > start && md.row_idx.back() == e.row) md.val.back() += e.v;
@@ -240,6 +322,47 @@ Model parse(const std::string& path, bool fixed) {
             }
             if ((section == "ROWS" || section == "COLUMNS") && !seen.insert(section).second)
                 throw ParseError("section " + section + " appears twice");
+            if (section == "COLUMNS" && !fixed) {  // the bulk of a file: tokenised in parallel, merged in order
+                size_t end = pos;
+                while (end < buf.size()) {
+                    size_t nl = buf.find('\n', end);
+                    if (nl == std::string::npos) nl = buf.size();
+                    std::string_view l(buf.data() + end, nl - end);
+                    if (!l.empty() && l.back() == '\r') l.remove_suffix(1);
+                    if (is_header(l)) break;
+                    end = nl + 1;
+                }
+                end = std::min(end, buf.size());
+                std::vector<std::vector<ColRec>> parts;
+                const int nt = int(std::max<size_t>(1, std::min<size_t>(size_t(host_threads()), (end - pos) >> 20)));
+                if (nt > 1 && tokenize_columns(buf, pos, end, nt, row_of, parts)) {
+                    for (const std::vector<ColRec>& part : parts)
+                    for (const ColRec& c : part) {
+                        if (c.kind) {
+                            in_int = c.kind == 1;
+                            continue;
+                        }
+                        int j;
+                        if (cur >= 0 && c.col == cur_name) {
+                            j = cur;
+                        } else {
+                            if (col_id.count(c.col))
+                                throw ParseError("column '" + std::string(c.col) + "' is listed in two separate blocks");
+                            close_column();
+                            j = int(md.col_names.size());
+                            col_id.add(c.col);
+                            md.col_names.emplace_back(c.col);
+                            cur_name = c.col;
+                            md.cost.push_back(0);
+                            md.is_int.push_back(in_int ? 1 : 0);
+                        }
+                        cur = j;
+                        if (c.row == -1) md.cost[j] += c.v;
+                        else if (c.row >= 0) pending.push_back({c.row, c.v});
+                    }
+                    pos = end;
+                }
+            }
             continue;
         }
         split(line, section, fixed, t);
@@ -256,7 +379,7 @@ Model parse(const std::string& path, bool fixed) {
                 if (obj_row.empty()) obj_row = std::string(t[1]);
                 else free_rows.insert(t[1]);
             } else if (type == 'E' || type == 'L' || type == 'G') {
-                row_id.insert(t[1], int(md.row_names.size()));
+                row_id.add(t[1]);
                 md.row_names.emplace_back(t[1]);
                 row_type.push_back(type);
             } else {
@@ -279,7 +402,7 @@ Model parse(const std::string& path, bool fixed) {
                     throw ParseError("column '" + std::string(t[0]) + "' is listed in two separate blocks");
                 close_column();
                 j = int(md.col_names.size());
-                col_id.insert(t[0], j);
+                col_id.add(t[0]);
                 md.col_names.emplace_back(t[0]);
                 cur_name = t[0];
                 md.cost.push_back(0);

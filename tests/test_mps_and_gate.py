@@ -188,3 +188,85 @@ def test_reader_matches_generator_roundtrip(engine_lib, tmp_path):
         for k in ("col_ptr", "row_idx", "val", "cost", "col_lo", "col_up", "row_lo", "row_up"):
             assert np.array_equal(getattr(m, k), getattr(lp, k)), (lp.name, k)
         assert m.obj_const == lp.obj_const and m.maximize == lp.maximize
+
+
+def _big_columns_text(lp, crlf=False):
+    """lp's MPS text with a COLUMNS section of several MB (parsed by the multi-threaded tokeniser) rewritten to
+    exercise every rule there: two entries per line, comments and blank lines, an integer MARKER block, a second N
+    row whose entries are dropped, and a duplicate (row, +v) (row, -v) pair that sums to zero and is dropped."""
+    head, rest = lp.mps_text().split("COLUMNS\n", 1)
+    cols, tail = rest.split("RHS\n", 1)
+    head = head.replace(" N OBJ\n", " N OBJ\n N FREE2\n", 1)
+    by_col = {}
+    for ln in cols.splitlines():
+        c, r, v = ln.split()
+        by_col.setdefault(c, []).append((r, v))
+    out, is_int = [], np.zeros(lp.n, np.uint8)
+    for j, (c, ents) in enumerate(by_col.items()):
+        if j == 100:
+            out.append("    MARKER                 'MARKER'                 'INTORG'")
+        if j == 200:
+            out.append("    MARKER                 'MARKER'                 'INTEND'")
+        if 100 <= j < 200:
+            is_int[j] = 1
+        if j % 997 == 0:
+            out += ["* a comment line", "   "]
+        if j % 5 == 1:
+            ents = ents + [("FREE2", "3.5")]
+        if j % 7 == 3:  # a row outside the column's own rows, +v then -v: the zero sum is dropped
+            rows = {r for r, _ in ents}
+            extra = next(f"R{i}" for i in range(lp.m) if f"R{i}" not in rows)
+            ents = [(extra, "1.25")] + ents + [(extra, "-1.25")]
+        for k in range(0, len(ents), 2):
+            pair = ents[k:k + 2]
+            out.append("    " + c + "".join(f"  {r}  {v}" for r, v in pair))
+    text = head + "COLUMNS\n" + "\n".join(out) + "\nRHS\n" + tail
+    return (text.replace("\n", "\r\n") if crlf else text), is_int
+
+
+@pytest.mark.parametrize("crlf", [False, True])
+def test_reader_parallel_columns_roundtrip(engine_lib, tmp_path, crlf):
+    """A COLUMNS section of several MB is tokenised on several threads and merged in file order: the model read
+    equals the generator's arrays exactly, integer markers included."""
+    lp = lpgen.general(8000, 24000, seed=5)
+    text, is_int = _big_columns_text(lp, crlf)
+    assert len(text) > 3 << 20
+    m = pdhg.read_mps(write(tmp_path, text))
+    for k in ("col_ptr", "row_idx", "val", "cost", "col_lo", "col_up", "row_lo", "row_up"):
+        assert np.array_equal(getattr(m, k), getattr(lp, k)), k
+    assert m.col_names == [f"X{j}" for j in range(lp.n)]
+    assert np.array_equal(m.is_int, is_int)
+
+
+@pytest.mark.parametrize("edit,msg", [
+    ("dup_late", "two separate blocks"),              # a closed column reopened near the end
+    ("dup_then_unknown_row", "two separate blocks"),  # the earlier error is the one reported
+    ("unknown_row_then_dup", "unknown row"),
+    ("bad_number_late", "bad number"),
+    ("bad_marker", "bad MARKER line"),
+])
+def test_reader_parallel_columns_errors(engine_lib, tmp_path, edit, msg):
+    """Errors in a multi-MB COLUMNS section are reported as the sequential reader reports them: the first one in
+    file order."""
+    lp = lpgen.general(8000, 24000, seed=5)
+    text, _ = _big_columns_text(lp)
+    lines = text.split("\n")
+    c0 = lines.index("COLUMNS")
+    c1 = lines.index("RHS")
+    late, early = c1 - 10, c0 + 50
+    if edit == "dup_late":
+        lines.insert(late, "    X5  R0  1")
+    elif edit == "dup_then_unknown_row":
+        lines.insert(late, "    X5  R0  1")
+        lines.insert(late + 5, "    " + lines[late + 5].split()[0] + "  NOSUCHROW  1")
+    elif edit == "unknown_row_then_dup":
+        lines.insert(late, "    X5  R0  1")
+        lines.insert(early, "    " + lines[early].split()[0] + "  NOSUCHROW  1")
+    elif edit == "bad_number_late":
+        lines.insert(late, "    " + lines[late].split()[0] + "  R0  1.2.3")
+    elif edit == "bad_marker":
+        lines.insert(late, "    MARKER  'MARKER'")
+    with pytest.raises(pdhg.TaralError) as e:
+        pdhg.read_mps(write(tmp_path, "\n".join(lines)))
+    free_msg = str(e.value).split(" (free format)")[0]
+    assert e.value.code == pdhg.ERR_PARSE and msg in free_msg, str(e.value)
