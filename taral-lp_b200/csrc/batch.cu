@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <map>
@@ -527,6 +528,9 @@ struct Batch final : BatchBase {
     int4 *A_it = nullptr, *Ae_it = nullptr, *T_it = nullptr, *Te_it = nullptr;
     int4 *A1_it = nullptr, *Ae1_it = nullptr, *T1_it = nullptr, *Te1_it = nullptr;
     std::vector<int4> h_a1, h_ap, h_t1, h_tp;  // host copies of the iteration block lists (autotuner)
+    std::vector<int4> h_ae1, h_ae, h_te1, h_te;  // and of their extensions (instance or pack of each entry)
+    std::vector<int4> c_a1, c_ae1, c_ap, c_ae, c_t1, c_te1, c_tp, c_te;  // the compacted lists last uploaded
+    bool compacted = false;
     int tuned[2] = {0, 0};
     int4 *A_ev = nullptr, *Ae_ev = nullptr, *T_ev = nullptr, *Te_ev = nullptr;
     int *rr = nullptr, *cr = nullptr, *slot_inst = nullptr;
@@ -784,6 +788,7 @@ struct Batch final : BatchBase {
         nA1 = int(a1_it.size()), nT1 = int(t1_it.size()), nAp = int(a_it.size()), nTp = int(t_it.size());
         A1_it = put(a1_it), Ae1_it = put(ae1_it), T1_it = put(t1_it), Te1_it = put(te1_it);
         h_a1 = a1_it, h_ap = a_it, h_t1 = t1_it, h_tp = t_it;
+        h_ae1 = ae1_it, h_ae = ae_it, h_te1 = te1_it, h_te = te_it;
         slot_inst = put(hslot), d_where = put(where);
         // 5. upload
         A_it = put(a_it), Ae_it = put(ae_it), T_it = put(t_it), Te_it = put(te_it);
@@ -920,6 +925,50 @@ struct Batch final : BatchBase {
         k_eval_finish<<<(ninst + 7) / 8, 256, 0, s>>>(ninst, d_where, rr, cr, partA, partT, act, dst);
         launches += 3;
     }
+    // The iteration lists of the running instances only. A stopped instance's CTAs would return at once, but in the
+    // tail of a batch they are most of the grid; dropping them changes no result: every running instance keeps all
+    // its entries in the same order, and a stopped instance is never touched again. The next block re-captures the
+    // graph with the smaller grids.
+    void upload_lists(const std::vector<int4>& a1, const std::vector<int4>& ae1, const std::vector<int4>& ap,
+                      const std::vector<int4>& ae, const std::vector<int4>& t1, const std::vector<int4>& te1,
+                      const std::vector<int4>& tp, const std::vector<int4>& te) {
+        auto up = [&](int4* d, const std::vector<int4>& h) {
+            if (!h.empty()) BK(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(int4), cudaMemcpyHostToDevice, s));
+        };
+        up(A1_it, a1), up(Ae1_it, ae1), up(A_it, ap), up(Ae_it, ae), up(T1_it, t1), up(Te1_it, te1), up(T_it, tp),
+            up(Te_it, te);
+        nA1 = int(a1.size()), nAp = int(ap.size()), nT1 = int(t1.size()), nTp = int(tp.size());
+        if (graph) {
+            BK(cudaGraphExecDestroy(graph));
+            graph = nullptr;
+        }
+    }
+    void compact_lists(const std::vector<int>& live) {
+        auto pick = [&](const std::vector<int4>& blk, const std::vector<int4>& ext, bool one, std::vector<int4>& ob,
+                        std::vector<int4>& oe) {
+            ob.clear(), oe.clear();
+            for (size_t k = 0; k < blk.size(); ++k) {
+                bool keep = false;
+                if (one) {
+                    keep = live[size_t(ext[k].x)] != 0;
+                } else {
+                    const Pack& q = packs[size_t(ext[k].x)];
+                    for (int t = 0; t < q.W; ++t) keep = keep || (q.inst[t] >= 0 && live[size_t(q.inst[t])] != 0);
+                }
+                if (keep) ob.push_back(blk[k]), oe.push_back(ext[k]);
+            }
+        };
+        pick(h_a1, h_ae1, true, c_a1, c_ae1), pick(h_ap, h_ae, false, c_ap, c_ae);
+        pick(h_t1, h_te1, true, c_t1, c_te1), pick(h_tp, h_te, false, c_tp, c_te);
+        upload_lists(c_a1, c_ae1, c_ap, c_ae, c_t1, c_te1, c_tp, c_te);
+        compacted = true;
+    }
+    void restore_lists() {
+        if (!compacted) return;
+        upload_lists(h_a1, h_ae1, h_ap, h_ae, h_t1, h_te1, h_tp, h_te);
+        compacted = false;
+    }
+
     void block(int steps) {
         if (nT) k_pack_xupd<T><<<nT, kThreads, 0, s>>>(T_ev, Te_ev, slot_inst, running, x, ATz, c, l, u, par, xs), ++launches;
         for (int k = 0; k < steps; ++k) {
@@ -943,6 +992,7 @@ struct Batch final : BatchBase {
     void solve(const double* const* x0, const double* const* y0, const double* w0, taral_outcome* outs,
                double* const* xo, double* const* yo) override {
         auto t0 = Clock::now();
+        restore_lists();  // a previous solve may have left the lists compacted
         cudaEvent_t e0, e1;
         BK(cudaEventCreate(&e0));
         BK(cudaEventCreate(&e1));
@@ -1047,6 +1097,12 @@ struct Batch final : BatchBase {
         k_set_deadline<<<1, 1, 0, s>>>(d_deadline, (unsigned long long)(left * 1e9));
         ++launches;
         int64_t it = 0;
+        // TARAL_COMPACT=0 keeps the full iteration lists; TARAL_TRACE=1 prints the running count per block
+        const char* ce = std::getenv("TARAL_COMPACT");
+        const bool compact = !(ce && std::atoi(ce) == 0);
+        const bool trace = std::getenv("TARAL_TRACE") != nullptr;
+        int live_lists = ninst;  // running instances when the lists were last built
+        std::vector<int> live(static_cast<size_t>(ninst));
         for (;;) {
             int steps = int(std::min<int64_t>(freq, opt.max_iter - it));
             if (steps <= 0) break;
@@ -1069,7 +1125,14 @@ struct Batch final : BatchBase {
             it += steps;
             BK(cudaMemcpyAsync(h_count, count, sizeof(int), cudaMemcpyDeviceToHost, s));
             BK(cudaStreamSynchronize(s));
+            if (trace) std::fprintf(stderr, "batch block it=%lld running=%d t=%.4f\n", (long long)it, *h_count, since(t0));
             if (*h_count == 0) break;
+            if (compact && 4 * int64_t(*h_count) <= 3 * int64_t(live_lists)) {
+                BK(cudaMemcpyAsync(live.data(), running, size_t(ninst) * sizeof(int), cudaMemcpyDeviceToHost, s));
+                BK(cudaStreamSynchronize(s));
+                compact_lists(live);
+                live_lists = *h_count;
+            }
         }
         BK(cudaGetLastError());
         // download

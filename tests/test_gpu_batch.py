@@ -96,3 +96,28 @@ def test_batch_packs_match_single_solves(engine_lib, monkeypatch, width):
         assert r["status"] == "near_optimal" and r["iterations"] == s["iterations"], (lp.name, r["iterations"], s["iterations"])
         assert rel(r["objective"], s["objective"]) < 1e-9
         assert np.max(np.abs(x - xsol)) <= 1e-9 * (1 + np.max(np.abs(xsol)))
+
+
+@pytest.mark.parametrize("pack", ["1", "8"])
+def test_batch_tail_compaction_changes_nothing(engine_lib, monkeypatch, pack):
+    """Instances stop at different iterations; once a quarter of the running ones have stopped, the iteration lists
+    are rebuilt without them. Compacted and full lists give identical counts and bit-identical points, and a second
+    solve on the same batch (lists restored) repeats the first."""
+    monkeypatch.setenv("TARAL_BATCH_PACK", pack)
+    base = lpgen.RefineryBase(3, seed=3)
+    pert = lpgen.perturbations(16, seed=7)
+    lps = [base.instance(2 + k % 2, pert[k]) for k in range(16)]
+    b = pdhg.Batch(lps, tol=1e-6, precision=pdhg.FP32, time_limit=300)
+    r1, x1, y1 = b.solve()
+    assert len({r["iterations"] for r in r1}) > 3  # the instances stop at different blocks
+    r2, x2, y2 = b.solve()
+    monkeypatch.setenv("TARAL_COMPACT", "0")
+    r3, x3, y3 = b.solve()
+    for a, c in ((r1, r2), (r1, r3)):
+        assert [r["iterations"] for r in a] == [r["iterations"] for r in c]
+        assert [r["objective"] for r in a] == [r["objective"] for r in c]
+    for xa, xb, xc in zip(x1, x2, x3):
+        assert np.array_equal(xa, xb) and np.array_equal(xa, xc)
+    for ya, yc in zip(y1, y3):
+        assert np.array_equal(ya, yc)
+    assert all(r["status"] == "near_optimal" for r in r1)
