@@ -211,6 +211,23 @@ def traffic_from_profile():
     return out
 
 
+def gather_floor(nnz):
+    """The random-gather floor of this GPU, measured now by the committed probe (bin/gather_probe: `nnz` int32 index +
+    float value pairs and one uniformly random float gather each, L2 flushed before every launch): {vector length:
+    microseconds per launch} for the vector lengths 500,000 (x, gathered by the row phase) and 200,000 (z, column
+    phase), or None when the probe is missing or fails."""
+    import subprocess
+    probe = ROOT / "taral-lp_b200" / "bin" / "gather_probe"
+    if not probe.exists():
+        return None
+    try:
+        out = subprocess.run([str(probe), str(int(nnz))], capture_output=True, text=True, timeout=300, check=True)
+        rows = [json.loads(line) for line in out.stdout.splitlines() if line.startswith("{")]
+        return {int(r["n"]): float(r["l2_gather_us"]) for r in rows}
+    except (subprocess.SubprocessError, OSError, ValueError, KeyError):
+        return None
+
+
 def our_arm(args, rank, world, dist):
     import torch
     import pdhg
@@ -280,6 +297,7 @@ def our_arm(args, rank, world, dist):
     dom = "row" if row_ms >= col_ms else "col"
     tr = traffic_from_profile()
     traffic = tr.get(dom) if tr else None
+    floor = gather_floor(nnz) if rank == 0 and (m, n) == (200_000, 500_000) else None
 
     if rank == 0:
         cpu = None
@@ -309,7 +327,13 @@ def our_arm(args, rank, world, dist):
                          "achieved": row_gbs if dom == "row" else col_gbs, "peak": peak, "unit": "GB/s",
                          "frac": (row_gbs if dom == "row" else col_gbs) / peak, "peak_kind": peak_kind,
                          "traffic": traffic, "row_ms": row_ms, "col_ms": col_ms,
-                         "bytes_per_launch": {"row": brow, "col": bcol}, "other_gbs": col_gbs if dom == "row" else row_gbs},
+                         "bytes_per_launch": {"row": brow, "col": bcol}, "other_gbs": col_gbs if dom == "row" else row_gbs,
+                         "gather_floor": None if not floor else {
+                             "row_us": floor.get(n), "col_us": floor.get(m),
+                             "row_frac": floor[n] / (row_ms * 1e3) if n in floor else None,
+                             "col_frac": floor[m] / (col_ms * 1e3) if m in floor else None,
+                             "source": "bin/gather_probe in this run: the same count of random 4-byte gathers "
+                                       "with their index/value stream, L2 flushed before each launch"}},
             "cpu_baseline": cpu,
             "gpu_launches": launches,
             "clocks": clk,

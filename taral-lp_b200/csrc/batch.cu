@@ -827,14 +827,13 @@ struct Batch final : BatchBase {
         tune();
     }
 
-    // Row-split autotuner (FP32 batches; the engine's three policies, per phase over the whole batch): a policy other
+    // Row-split autotuner (FP32 batches; the engine's five policies, per phase over the whole batch): a policy other
     // than the hybrid rule is kept only if it is at least 5 % faster. TARAL_TUNE=0 keeps the hybrid rule.
     void tune() {
         if (sizeof(T) != sizeof(float)) return;
         if (const char* e = std::getenv("TARAL_TUNE"))
             if (std::atoi(e) == 0) return;
-        int forced = -1;  // TARAL_ROWSPLIT=0|1|2: that policy, untimed
-        if (const char* e = std::getenv("TARAL_ROWSPLIT")) forced = std::max(0, std::min(2, std::atoi(e)));
+        const int forced = forced_row_split();  // that policy, untimed
         if (forced < 0 && nnz_total < (int64_t(1) << 20)) return;  // small: timings are noise
         std::vector<int> ones(size_t(ninst), 1);
         BK(cudaMemcpyAsync(pactive, ones.data(), ones.size() * sizeof(int), cudaMemcpyHostToDevice, s));
@@ -842,10 +841,7 @@ struct Batch final : BatchBase {
         BK(cudaMemsetAsync(pw, 0, size_t(M) * sizeof(T), s));
         auto variant = [](const std::vector<int4>& h, int policy, bool& any) {
             std::vector<int4> a(h);
-            for (int4& b : a) {
-                if (policy == 1 && (b.y & kUniformCandidate)) b.y |= kUniformRows, any = true;
-                if (policy == 2) b.y |= kSegmented, any = true;
-            }
+            if (policy > 0 && apply_row_split(a, policy)) any = true;
             return a;
         };
         for (int phase = 0; phase < 2; ++phase) {
@@ -876,15 +872,15 @@ struct Batch final : BatchBase {
                 cudaEventDestroy(e0), cudaEventDestroy(e1);
                 return ms;
             };
-            std::vector<int4> v1[3], vp[3];
-            float t[3] = {0, 1e30f, 1e30f};
-            for (int pol = 0; pol < 3; ++pol) {
+            std::vector<int4> v1[kPolicies], vp[kPolicies];
+            float t[kPolicies] = {0, 1e30f, 1e30f, 1e30f, 1e30f};
+            for (int pol = 0; pol < kPolicies; ++pol) {
                 bool any = pol == 0;
                 v1[pol] = variant(h1, pol, any), vp[pol] = variant(hp, pol, any);
                 if (any && forced < 0) t[pol] = time_lists(v1[pol], vp[pol]);
             }
             int best = 0;
-            for (int k = 1; k < 3; ++k)
+            for (int k = 1; k < kPolicies; ++k)
                 if (t[k] < 0.95f * t[0] && t[k] < t[best]) best = k;
             if (forced >= 0) best = forced;
             tuned[phase] = best;

@@ -52,6 +52,24 @@ void keep_pool_memory(int dev) {
 // its own (block_sums sums it with the whole CTA).
 std::vector<int4> build_row_blocks(const int64_t* ptr, int rows) { return build_row_blocks(ptr, rows, kTile, kRowsMax); }
 
+// Policies: 0 the hybrid rule, 1 a thread per row in kUniformCandidate blocks, 2 segmented sums in every block, 3
+// 8-lane groups for rows up to kMid nonzeros in every block, 4 policies 1 and 3 together.
+bool apply_row_split(std::vector<int4>& blk, int policy) {
+    bool changed = false;
+    for (int4& b : blk) {
+        const bool cand = (b.y & kUniformCandidate) != 0;
+        if ((policy == 1 || policy == 4) && cand) b.y |= kUniformRows, changed = true;
+        if (policy == 2) b.y |= kSegmented, changed = true;
+        if (policy == 3 || policy == 4) b.y |= kMidGroups, changed = changed || policy == 3;
+    }
+    return changed;
+}
+
+int forced_row_split() {
+    const char* e = std::getenv("TARAL_ROWSPLIT");
+    return e ? std::max(0, std::min(kPolicies - 1, std::atoi(e))) : -1;
+}
+
 std::vector<int4> build_row_blocks(const int64_t* ptr, int rows, int tile, int rows_max) {
     std::vector<int4> out;
     auto close = [&](int r0, int r1) {  // y: rows | kUniformCandidate when no row is much longer than the mean
@@ -294,14 +312,14 @@ struct Engine final : EngineBase {
     // Row-split policy per matrix (FP32 contexts, matrices of at least 2^20 nonzeros), timed on the matrix itself
     // (CUDA-event time of 10 SpMV launches after 3 warm-ups): 0 the hybrid rule (thread per row up to 48 nonzeros,
     // warp per longer row), 1 thread per row in the kUniformCandidate blocks, 2 the balanced segmented sums
-    // (kSegmented) in every block. A policy other than 0 is kept only if it is at least 5 % faster. FP64 contexts
+    // (kSegmented) in every block, 3 the hybrid rule with 8-lane groups for rows up to 128 nonzeros (kMidGroups),
+    // 4 policies 1 and 3 together. A policy other than 0 is kept only if it is at least 5 % faster. FP64 contexts
     // keep policy 0 (the parity pins' summation order); TARAL_TUNE=0 keeps it everywhere.
     void tune() {
         if (sizeof(T) != sizeof(float)) return;
         if (const char* e = std::getenv("TARAL_TUNE"))
             if (std::atoi(e) == 0) return;
-        int forced = -1;  // TARAL_ROWSPLIT=0|1|2: that policy for every matrix, untimed (tests, experiments)
-        if (const char* e = std::getenv("TARAL_ROWSPLIT")) forced = std::max(0, std::min(2, std::atoi(e)));
+        const int forced = forced_row_split();  // that policy for every matrix, untimed (tests, experiments)
         int which = 0;
         for (DevMat* d : {&A, &AT}) {
             const int slot = which++;
@@ -309,11 +327,9 @@ struct Engine final : EngineBase {
             std::vector<int4> base(size_t(d->nblk));
             CK(cudaMemcpyAsync(base.data(), d->blk, base.size() * sizeof(int4), cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));
-            std::vector<std::vector<int4>> cand(3, base);
-            bool uni = false;
-            for (int4& b : cand[1])
-                if (b.y & kUniformCandidate) b.y |= kUniformRows, uni = true;
-            for (int4& b : cand[2]) b.y |= kSegmented;
+            std::vector<std::vector<int4>> cand(kPolicies, base);
+            bool differs[kPolicies] = {true};
+            for (int k = 1; k < kPolicies; ++k) differs[k] = apply_row_split(cand[k], k);
             const T* xin = d == &A ? pv : pw;  // scratch vectors of the right length (power iteration)
             T* yout = d == &A ? pw : pu;
             auto time_list = [&](const std::vector<int4>& list) {
@@ -336,8 +352,9 @@ struct Engine final : EngineBase {
             if (forced >= 0) {
                 best = forced;
             } else {
-                float t[3] = {time_list(cand[0]), uni ? time_list(cand[1]) : 1e30f, time_list(cand[2])};
-                for (int k = 1; k < 3; ++k)
+                float t[kPolicies];
+                for (int k = 0; k < kPolicies; ++k) t[k] = differs[k] ? time_list(cand[k]) : 1e30f;
+                for (int k = 1; k < kPolicies; ++k)
                     if (t[k] < 0.95f * t[0] && t[k] < t[best]) best = k;
             }
             tuned[slot] = best;
@@ -751,6 +768,7 @@ extern "C" int taral_spmv_plan_create(int rows, int cols, const int64_t* host_pt
         if (host_ptr[r + 1] < host_ptr[r]) return TARAL_ERR_INPUT;
     if (host_ptr[rows] > INT32_MAX - 64) return TARAL_ERR_INPUT;
     std::vector<int4> blk = taral::build_row_blocks(host_ptr, rows);
+    if (taral::forced_row_split() > 0) taral::apply_row_split(blk, taral::forced_row_split());  // tests
     auto* p = new taral_spmv_plan;
     p->rows = rows, p->cols = cols, p->dtype = dtype, p->nblk = int(blk.size());
     if (cudaMalloc(&p->blk, std::max<size_t>(blk.size(), 1) * sizeof(int4)) != cudaSuccess) {

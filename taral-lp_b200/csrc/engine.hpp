@@ -46,6 +46,10 @@ std::vector<int4> build_row_blocks(const int64_t* ptr, int rows);
 void keep_pool_memory(int dev);  // the device pool keeps freed memory for reuse by later contexts
 // Blocks of at most `tile` nonzeros and `rows_max` rows (a longer row is a block of its own).
 std::vector<int4> build_row_blocks(const int64_t* ptr, int rows, int tile, int rows_max);
+// The block list with the flags of row-split policy 0..4 (kernels.cuh, kPolicies); returns false when the policy
+// changes nothing on this list (no block it applies to).
+bool apply_row_split(std::vector<int4>& blk, int policy);
+int forced_row_split();  // TARAL_ROWSPLIT (0..4) when set, else -1
 // Set-up from the column-wise model with the scaling done on the device, bit-identical to the reference's: P gets
 // Dr, Dc, the scaled vectors and the norms (its matrices stay empty); host_s: seconds of host work.
 struct Scaled;

@@ -138,6 +138,12 @@ constexpr int kUniformCandidate = 1 << 17;
 //               autotuner on FP32 matrices when it is measurably faster.
 constexpr int kSegmented = 1 << 18;
 constexpr int kSeg = 8;
+// kMidGroups -- rows of kShort + 1 .. kMid nonzeros are summed by groups of kGroup lanes (four rows per warp, lanes
+//               strided by kGroup, a three-level shuffle tree) instead of a whole warp each. Set by the autotuner.
+constexpr int kMidGroups = 1 << 19;
+constexpr int kMid = 128;
+constexpr int kGroup = 8;
+constexpr int kPolicies = 5;  // row-split policies the autotuners choose from (0 = the hybrid rule)
 static_assert(kSeg * kThreads >= kTile, "kSeg products per thread must cover a block");
 constexpr int kQuads = (kTile + 3 + 3) / 4 / kThreads;  // 16-byte quads per thread in the staging loop (2)
 static_assert(kQuads * 4 * kThreads >= kTile + 3, "a block's quads must fit the staging loop");
@@ -168,7 +174,8 @@ struct RowSmem {
     double rowsum[kRowsMax];
     int rptr[kRowsMax + 1];
     short longrow[kRowsMax];
-    int nlong;
+    short midrow[kRowsMax];
+    int nlong, nmid;
     double segv[kThreads / 32];  // segmented scan: per-warp carry value and flag
     int segf[kThreads / 32];
 };
@@ -278,7 +285,7 @@ __device__ __forceinline__ void block_sums(const int* __restrict__ ptr, const in
     const bool seg = (meta.y & kSegmented) != 0;
     const int base = seg ? (p0 & ~3) : p0;
     for (int t = tid; t <= nrows; t += kThreads) sm.rptr[t] = ptr[r0 + t] - base;
-    if (tid == 0) sm.nlong = 0;
+    if (tid == 0) sm.nlong = 0, sm.nmid = 0;
     if (seg)  // rows without entries stay zero; every other row is written once, after the barrier
         for (int t = tid; t < nrows; t += kThreads) sm.rowsum[t] = 0;
     if (VEC) {
@@ -334,8 +341,10 @@ __device__ __forceinline__ void block_sums(const int* __restrict__ ptr, const in
         segmented_sums(sm, nrows);
         return;
     }
-    // 2. reduce: short rows (every row of a uniform block) by their own thread, long rows by a warp each
+    // 2. reduce: short rows (every row of a uniform block) by their own thread, long rows by a warp each (with
+    //    kMidGroups: rows up to kMid nonzeros by kGroup lanes each)
     const int thread_max = (meta.y & kUniformRows) ? kTile : kShort;
+    const int mid_max = (meta.y & kMidGroups) ? kMid : thread_max;
     if (tid < nrows) {
         const int a = sm.rptr[tid], b = sm.rptr[tid + 1];
         if (b - a <= thread_max) {
@@ -350,11 +359,27 @@ __device__ __forceinline__ void block_sums(const int* __restrict__ ptr, const in
             }
             for (; k < b; ++k) s += double(sm.prod[pidx(k)]);
             sm.rowsum[tid] = s;
+        } else if (b - a <= mid_max) {
+            sm.midrow[atomicAdd(&sm.nmid, 1)] = short(tid);
         } else {
             sm.longrow[atomicAdd(&sm.nlong, 1)] = short(tid);
         }
     }
     __syncthreads();
+    {  // rows of the mid list: group g of a warp takes list entry base + g; warp-uniform trip count
+        const int grp = lane / kGroup, gl = lane % kGroup;
+        for (int base = warp * (32 / kGroup); base < sm.nmid; base += kThreads / kGroup) {
+            const int i = base + grp;
+            double s = 0;
+            if (i < sm.nmid) {
+                const int t = sm.midrow[i];
+                for (int k = sm.rptr[t] + gl; k < sm.rptr[t + 1]; k += kGroup) s += double(sm.prod[pidx(k)]);
+            }
+#pragma unroll
+            for (int off = kGroup / 2; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+            if (i < sm.nmid && gl == 0) sm.rowsum[sm.midrow[i]] = s;
+        }
+    }
     for (int i = warp; i < sm.nlong; i += kThreads / 32) {  // warp-uniform trip count: all lanes shuffle
         const int t = sm.longrow[i];
         double s = 0;

@@ -146,11 +146,12 @@ def test_kernel_launch_count(engine_lib, oracle_lib):
     assert eng.kernel_launches - before == 2 * (1 + 2 * 64)
 
 
-@pytest.mark.parametrize("policy", ["0", "1", "2"])
+@pytest.mark.parametrize("policy", ["0", "1", "2", "3", "4"])
 def test_row_split_policies_agree(engine_lib, monkeypatch, policy):
-    # the three row-split policies of the autotuner (hybrid, thread per row in uniform blocks, balanced segmented
-    # sums) on a Zipf LP whose long rows span many threads of a block: each reaches the tolerance at the same
-    # objective (they differ only in the FP64 summation order of the products)
+    # the five row-split policies of the autotuner (hybrid, thread per row in uniform blocks, balanced segmented
+    # sums, 8-lane groups for rows of 49..128 nonzeros, uniform blocks plus groups) on a Zipf LP whose long rows span
+    # many threads of a block: each reaches the tolerance at the same objective (they differ only in the FP64
+    # summation order of the products)
     monkeypatch.setenv("TARAL_ROWSPLIT", policy)
     lp = lpgen.planted(20_000, 50_000, 10, seed=4, zipf=1.2, cap=2000, floor=5)
     r, x, _ = pdhg.solve(lp, tol=1e-6, precision=pdhg.FP32, time_limit=120)
