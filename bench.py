@@ -128,6 +128,44 @@ def ref_binary():
     return ROOT / "oracle" / "_ref" / "pdhg"
 
 
+def cpu_solvers(cap_s=120.0):
+    """The reference's own CPU dual simplex and IPM (single-threaded engines of `oracle/_ref/taral`, each capped at
+    cap_s seconds) and this engine on the small planted LP (2,000 x 5,000, 5 nonzeros per column, seed 1), timed
+    in this run on this host, with the objective errors against the planted optimum. A reported baseline only."""
+    import lpgen
+    import pdhg
+    taral = ROOT / "oracle" / "_ref" / "taral"
+    if not taral.exists():
+        return None
+    lp = lpgen.planted(2000, 5000, 5, seed=1)
+    out = {"workload": "planted LP m=2000 n=5000, 5 nonzeros per column, seed 1, tol 1e-6", "cores": 1,
+           "cap_s": cap_s, "planted_objective": lp.obj_star}
+    with tempfile.TemporaryDirectory() as td:
+        f, j = Path(td) / "p.mps", Path(td) / "p.json"
+        lp.write_mps(f)
+        for method in ("ipm", "dual"):
+            t0 = time.perf_counter()
+            try:
+                subprocess.run([str(taral), str(f), "--method", method, "--time-limit", str(cap_s), "--json", str(j)],
+                               check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL, timeout=cap_s + 60)
+                rep = json.loads(j.read_text())
+                out[method] = {"s": time.perf_counter() - t0, "status": rep.get("status"),
+                               "objective_rel_err": abs(rep["objective"] - lp.obj_star) / abs(lp.obj_star)}
+            except (subprocess.SubprocessError, OSError, ValueError, KeyError) as e:
+                out[method] = {"s": time.perf_counter() - t0, "status": f"failed: {type(e).__name__}"}
+    for name, prec in (("gpu_pdhg_fp32", pdhg.FP32), ("gpu_pdhg_fp64", pdhg.FP64)):
+        pdhg.solve(lp, tol=1e-6, precision=prec)  # untimed first call
+        ts, r = [], None
+        for _ in range(3):
+            t0 = time.perf_counter()
+            r, _, _ = pdhg.solve(lp, tol=1e-6, precision=prec)
+            ts.append(time.perf_counter() - t0)
+        out[name] = {"s": sorted(ts)[1], "status": r["status"], "iterations": r["iterations"],
+                     "objective_rel_err": abs(r["objective"] - lp.obj_star) / abs(lp.obj_star),
+                     "what": "taral_pdhg_solve from host arrays, median of 3"}
+    return out
+
+
 def run_reference_sample(lp, iters, threads):
     """The reference CPU PDHG (--device cpu, FP64) on the model for `iters` iterations; per-iteration seconds."""
     with tempfile.TemporaryDirectory() as td:
@@ -216,7 +254,6 @@ def gather_floor(nnz):
     float value pairs and one uniformly random float gather each, L2 flushed before every launch): {vector length:
     microseconds per launch} for the vector lengths 500,000 (x, gathered by the row phase) and 200,000 (z, column
     phase), or None when the probe is missing or fails."""
-    import subprocess
     probe = ROOT / "taral-lp_b200" / "bin" / "gather_probe"
     if not probe.exists():
         return None
@@ -309,6 +346,7 @@ def our_arm(args, rank, world, dist):
                    "kind": "reference",
                    "sample": f"{REF_SAMPLE_ITERS} iterations of the reference CPU PDHG (FP64, {threads} threads) "
                              f"on this LP, projected to the {n_it} FP64 iterations to 1e-6 plus its setup"}
+        solvers = cpu_solvers() if world == 1 and not args.no_cpu_baseline else None
         r0 = outs[-1]
         line = {
             "metric": METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": args.steps,
@@ -335,6 +373,7 @@ def our_arm(args, rank, world, dist):
                              "source": "bin/gather_probe in this run: the same count of random 4-byte gathers "
                                        "with their index/value stream, L2 flushed before each launch"}},
             "cpu_baseline": cpu,
+            "cpu_solvers_small_lp": solvers,
             "gpu_launches": launches,
             "clocks": clk,
         }

@@ -118,7 +118,7 @@ int solve_model(const taral_model& md, const Options& o, SolveResult& res, const
     const double release_s = since(t);
     if (std::getenv("TARAL_TIMING"))
         std::fprintf(stderr, "taral: scale %.4f s, transfer %.4f s, solve %.4f s, finish %.4f s, release %.4f s, "
-                     "thread-per-row A %d A^T %d\n", res.scale_s, res.transfer_s, res.solve_s, finish_s, release_s,
+                     "row-split policy A %d A^T %d\n", res.scale_s, res.transfer_s, res.solve_s, finish_s, release_s,
                      tuned_a, tuned_t);
     res.m = P.m, res.n = P.n;
     return TARAL_OK;
