@@ -14,11 +14,14 @@ tolerance 1e-6, seeded synthetic data (seed = rank). One step = one full solve o
 
 Also reported: the roofline of the dominant kernel (mean CUDA-event duration of the row-phase and column-phase
 kernels launched one at a time on the engine stream, algorithmic bytes per launch, against the measured HBM
-copy bandwidth), the reference's own CPU PDHG timed on a bounded sample on this host, SM clocks sampled during
-the timed region, and the number of engine kernels launched in it.
+copy bandwidth) beside the random-gather floor measured in the same run, the reference's own CPU PDHG timed on a
+bounded sample on this host (and its CPU IPM and dual simplex on a small planted LP), SM clocks sampled during the
+timed region, and the number of engine kernels launched in it.
 
   python bench.py [--gpus N] [--steps K] [--warmup W]        our engine
-  python bench.py --impl reference ...                       the reference CPU PDHG (oracle/_ref/pdhg)
+  python bench.py --impl reference ...                       the reference CPU PDHG (oracle/_ref/pdhg), plus its GPU
+                                                             backend on the same LP (--no-reference-gpu skips it)
+  python bench.py [--impl reference] --workload ledger       the reference's published workloads, FP64 (either arm)
   python bench.py --profile-blocks B                         ncu capture mode: B blocks of 64 steps, no report
   python bench.py --workload family [--instances 512]        the batched scenario family against the plain engine
   python bench.py --workload family --profile-blocks B       ncu capture mode of the batched engine (16 scenarios)
@@ -180,6 +183,23 @@ def run_reference_sample(lp, iters, threads):
     return per_it, setup, rep
 
 
+def run_reference_gpu(lp, limit_s=120.0):
+    """The reference's own GPU backend (oracle/_ref/pdhg --device gpu, its default FP64, built for sm_100a from its
+    sources) on the model to 1e-6, capped at limit_s: its JSON report, or {"status": "failed: ..."}."""
+    with tempfile.TemporaryDirectory() as td:
+        f, j = Path(td) / "m.mps", Path(td) / "r.json"
+        lp.write_mps(f)
+        try:
+            subprocess.run([str(ref_binary()), str(f), "--device", "gpu", "--tol", "1e-6", "--time-limit", str(limit_s),
+                            "--json", str(j)], check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL,
+                           timeout=limit_s + 300)
+            rep = json.loads(j.read_text())
+        except (subprocess.SubprocessError, OSError, ValueError) as e:
+            return {"status": f"failed: {type(e).__name__}"}
+    return {k: rep.get(k) for k in ("status", "iterations", "restarts", "objective", "setup_s", "solve_s", "total_s",
+                                    "precision", "device")}
+
+
 REF_BENCH_LP = ROOT / "tests" / "golden" / "reference_bench_lp.json"
 
 
@@ -220,6 +240,9 @@ def reference_arm(args, rank, world):
                        "l2": "n/a (CPU)", "fp64_iterations_to_tol": n_it, "fp64_status": st},
             "cpu_baseline": {"value": v, "unit": "s", "cores": threads, "kind": "reference", "sample": sample},
             "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if not args.no_reference_gpu:  # beside the CPU arm: the reference's GPU backend on the same LP and GPU, untimed here
+        line["gpu_backend"] = {"what": "the reference's own GPU PDHG (--device gpu, FP64: its FP32 mode does not reach "
+                                       "1e-6 on this LP) on the same LP, one run", **run_reference_gpu(lp)}
     print(json.dumps(line))
 
 
@@ -346,7 +369,7 @@ def our_arm(args, rank, world, dist):
                    "kind": "reference",
                    "sample": f"{REF_SAMPLE_ITERS} iterations of the reference CPU PDHG (FP64, {threads} threads) "
                              f"on this LP, projected to the {n_it} FP64 iterations to 1e-6 plus its setup"}
-        solvers = cpu_solvers() if world == 1 and not args.no_cpu_baseline else None
+        solvers = cpu_solvers() if cpu is not None else None  # the reference CPU solvers on the small LP
         r0 = outs[-1]
         line = {
             "metric": METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": args.steps,
@@ -372,12 +395,46 @@ def our_arm(args, rank, world, dist):
                              "col_frac": floor[m] / (col_ms * 1e3) if m in floor else None,
                              "source": "bin/gather_probe in this run: the same count of random 4-byte gathers "
                                        "with their index/value stream, L2 flushed before each launch"}},
-            "cpu_baseline": cpu,
-            "cpu_solvers_small_lp": solvers,
+            "cpu_baseline": cpu if cpu is None or solvers is None else {**cpu, "solvers_small_lp": solvers},
             "gpu_launches": launches,
             "clocks": clk,
         }
         print(json.dumps(line))
+
+
+# The reference's own published GPU workloads (gpu/gen_lp.py models, reproduced byte for byte by lpgen), FP64 to
+# 1e-6, with the iteration counts of its ledgers (results/gpu_pdhg/synth_packing_tol1e-6.csv:12,
+# synth_transport_tol1e-6.csv:12) and its published solve times on an RTX 5050 laptop GPU.
+LEDGER = {"packing_1M": (lambda lpgen: lpgen.packing(1_000_000), 6848, 23.70),
+          "transport_1000x1000": (lambda lpgen: lpgen.transport(1000, 1000), 73344, 35.41)}
+
+
+def ledger_arm(args, reference):
+    """`--workload ledger`: the reference's published PDHG workloads on this GPU, FP64 to 1e-6 (their ledger
+    precision). Ours: `taral_pdhg_solve` from host arrays (median of `--steps` after one untimed call), FP64 and FP32.
+    Reference (`--impl reference`): its own GPU backend, `oracle/_ref/pdhg --device gpu`, one run each."""
+    import lpgen
+    out = {}
+    for name, (make, ledger_it, published_s) in LEDGER.items():
+        lp = make(lpgen)
+        row = {"ledger_iterations": ledger_it, "published_solve_s_rtx5050": published_s}
+        if reference:
+            row["reference_gpu_fp64"] = run_reference_gpu(lp, limit_s=600.0)
+        else:
+            import pdhg
+            for tag, prec in (("fp64", pdhg.FP64), ("fp32", pdhg.FP32)):
+                pdhg.solve(lp, tol=1e-6, precision=prec)
+                ts, r = [], None
+                for _ in range(max(args.steps, 1)):
+                    t0 = time.perf_counter()
+                    r, _, _ = pdhg.solve(lp, tol=1e-6, precision=prec)
+                    ts.append(time.perf_counter() - t0)
+                row[tag] = {"e2e_s": statistics.median(ts), "solve_s": r["solve_s"], "iterations": r["iterations"],
+                            "status": r["status"], "objective": r["objective"]}
+        out[name] = row
+        print(json.dumps({name: row}), file=sys.stderr, flush=True)
+    print(json.dumps({"impl": "reference" if reference else "ours", "workload": "ledger", "tol": 1e-6,
+                      "models": out}))
 
 
 def family_lps(count, seed=2024):
@@ -521,9 +578,11 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--profile-blocks", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["lp", "family", "warmstart"], default="lp",
+    ap.add_argument("--no-reference-gpu", action="store_true", help="reference arm: skip its GPU backend run")
+    ap.add_argument("--workload", choices=["lp", "family", "warmstart", "ledger"], default="lp",
                     help="lp: the single large LP (the bench line); family: the batched scenario family; "
-                         "warmstart: the learned warm start on the 24-period family")
+                         "warmstart: the learned warm start on the 24-period family; ledger: the reference's "
+                         "published PDHG workloads (both arms)")
     ap.add_argument("--instances", type=int, default=512)
     ap.add_argument("--sample", type=int, default=12)
     ap.add_argument("--train", type=int, default=512)
@@ -532,6 +591,10 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     dist = world > 1
+    if args.workload == "ledger":
+        if rank == 0:
+            ledger_arm(args, args.impl == "reference")
+        return
     if args.impl == "reference":
         reference_arm(args, rank, world)
         return
