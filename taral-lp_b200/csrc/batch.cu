@@ -74,8 +74,6 @@ constexpr int kPairs = (kTile + 4 + kThreads - 1) / kThreads;  // staged pairs p
 static_assert((pack_tile(8) + 3) * 8 <= kPairs * kThreads && (pack_tile(1) + 3) <= kPairs * kThreads, "pairs");
 
 __device__ __forceinline__ int log2w(int W) { return W >= 8 ? 3 : W >= 4 ? 2 : W >= 2 ? 1 : 0; }
-__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
-__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
 
 template <class P>
 struct PackSmem {
@@ -478,6 +476,7 @@ struct Shared {  // one distinct scaled matrix
     int pbaseA = 0, pbaseT = 0;
     int64_t nnzbase = 0, nnz = 0;
     int dr_off = 0, dc_off = 0;  // offsets of this matrix's Dr / Dc in the device scaling scratch
+    int maxrowA = 0, maxrowT = 0;  // longest row of A and of A^T
 };
 
 uint64_t fnv(const void* p, size_t n, uint64_t h) {  // FNV-1a over 8-byte words, then the tail bytes
@@ -532,6 +531,7 @@ struct Batch final : BatchBase {
     std::vector<int4> c_a1, c_ae1, c_ap, c_ae, c_t1, c_te1, c_tp, c_te;  // the compacted lists last uploaded
     bool compacted = false;
     int tuned[2] = {0, 0};
+    bool thread1[2] = {false, false};  // width-1 lists of A / A^T run on k_rowthread_batch
     int4 *A_ev = nullptr, *Ae_ev = nullptr, *T_ev = nullptr, *Te_ev = nullptr;
     int *rr = nullptr, *cr = nullptr, *slot_inst = nullptr;
     int2* d_where = nullptr;
@@ -736,6 +736,10 @@ struct Batch final : BatchBase {
                 u0 += size_t(used);
             }
             Shared& shw = *mats[k];
+            for (int r = 0; r < shw.S.m; ++r)
+                shw.maxrowA = std::max<int>(shw.maxrowA, int(shw.S.A.ptr[size_t(r) + 1] - shw.S.A.ptr[size_t(r)]));
+            for (int r = 0; r < shw.S.n; ++r)
+                shw.maxrowT = std::max<int>(shw.maxrowT, int(shw.S.AT.ptr[size_t(r) + 1] - shw.S.AT.ptr[size_t(r)]));
             for (int p : packs_of[k]) {
                 const int W = packs[p].W;
                 if (!shw.blk.count(W))
@@ -827,18 +831,24 @@ struct Batch final : BatchBase {
         tune();
     }
 
-    // Row-split autotuner (FP32 batches; the engine's five policies, per phase over the whole batch): a policy other
-    // than the hybrid rule is kept only if it is at least 5 % faster. TARAL_TUNE=0 keeps the hybrid rule.
+    // Autotuner, per phase over the whole batch (batches of at least 2^20 nonzeros), timed on the phase itself with
+    // its fused step (5 launches after 2 warm-ups, on the not yet started state: solve() rewrites every vector the
+    // steps write); a choice other than the default is kept only if it is at least 5 % faster:
+    // 1. FP32 batches: the engine's five row-split policies (policies 1, 3, 4 only where some row exceeds kShort);
+    // 2. any precision, phases whose matrices have no row over kShort nonzeros: k_rowthread_batch for the width-1
+    //    lists (bit-identical under policy 0).
+    // TARAL_TUNE=0 keeps the defaults; TARAL_ROWSPLIT=0..4 and TARAL_ROWTHREAD=0|1 force a choice, untimed.
     void tune() {
-        if (sizeof(T) != sizeof(float)) return;
         if (const char* e = std::getenv("TARAL_TUNE"))
             if (std::atoi(e) == 0) return;
-        const int forced = forced_row_split();  // that policy, untimed
-        if (forced < 0 && nnz_total < (int64_t(1) << 20)) return;  // small: timings are noise
+        const int forced = forced_row_split();
+        int forced_thread = -1;
+        if (const char* e = std::getenv("TARAL_ROWTHREAD")) forced_thread = std::atoi(e) != 0 ? 1 : 0;
+        const bool timing = forced < 0 && forced_thread < 0;
+        if (timing && nnz_total < (int64_t(1) << 20)) return;  // small: timings are noise
         std::vector<int> ones(size_t(ninst), 1);
         BK(cudaMemcpyAsync(pactive, ones.data(), ones.size() * sizeof(int), cudaMemcpyHostToDevice, s));
-        BK(cudaMemsetAsync(pv, 0, size_t(N) * sizeof(T), s));
-        BK(cudaMemsetAsync(pw, 0, size_t(M) * sizeof(T), s));
+        BK(cudaMemsetAsync(par, 0, 2 * size_t(ninst) * sizeof(double), s));
         auto variant = [](const std::vector<int4>& h, int policy, bool& any) {
             std::vector<int4> a(h);
             if (policy > 0 && apply_row_split(a, policy)) any = true;
@@ -849,17 +859,19 @@ struct Batch final : BatchBase {
             std::vector<int4>& hp = phase ? h_tp : h_ap;
             int4* d1 = phase ? T1_it : A1_it;
             int4* dp = phase ? T_it : A_it;
+            int maxrow = 0;
+            for (const auto& m : mats) maxrow = std::max(maxrow, phase ? m->maxrowT : m->maxrowA);
+            const bool short_rows = maxrow <= kShort;
             auto put_lists = [&](const std::vector<int4>& l1, const std::vector<int4>& lp) {
                 if (!l1.empty()) BK(cudaMemcpyAsync(d1, l1.data(), l1.size() * sizeof(int4), cudaMemcpyHostToDevice, s));
                 if (!lp.empty()) BK(cudaMemcpyAsync(dp, lp.data(), lp.size() * sizeof(int4), cudaMemcpyHostToDevice, s));
             };
             auto run = [&] {
-                if (phase) spmv_T(pw, EpiStore<T>{pu}, pactive);
-                else spmv_A(pv, EpiStore<T>{pw}, pactive);
+                if (phase) spmv_T(z, EpiCol<T>{ATz, x, xs, c, l, u, par, 1}, pactive);
+                else spmv_A(x, EpiRow<T>{Ax, z, zs, rl, ru, par}, pactive);
             };
-            auto time_lists = [&](const std::vector<int4>& l1, const std::vector<int4>& lp) {
-                put_lists(l1, lp);
-                for (int r = 0; r < 2; ++r) run();
+            auto time_run = [&](int warm) {
+                for (int r = 0; r < warm; ++r) run();
                 cudaEvent_t e0, e1;
                 BK(cudaEventCreate(&e0));
                 BK(cudaEventCreate(&e1));
@@ -873,17 +885,37 @@ struct Batch final : BatchBase {
                 return ms;
             };
             std::vector<int4> v1[kPolicies], vp[kPolicies];
-            float t[kPolicies] = {0, 1e30f, 1e30f, 1e30f, 1e30f};
+            bool timed[kPolicies] = {true};
             for (int pol = 0; pol < kPolicies; ++pol) {
                 bool any = pol == 0;
                 v1[pol] = variant(h1, pol, any), vp[pol] = variant(hp, pol, any);
-                if (any && forced < 0) t[pol] = time_lists(v1[pol], vp[pol]);
+                if (pol > 0) timed[pol] = sizeof(T) == sizeof(float) && any && (!short_rows || pol == 2);
             }
             int best = 0;
-            for (int k = 1; k < kPolicies; ++k)
-                if (t[k] < 0.95f * t[0] && t[k] < t[best]) best = k;
-            if (forced >= 0) best = forced;
+            bool thread = false;
+            if (!timing) {
+                if (sizeof(T) == sizeof(float) && forced >= 0) best = forced;
+                thread = short_rows && best == 0 && forced_thread == 1;
+            } else {
+                put_lists(v1[0], vp[0]);
+                const float t0 = time_run(6);
+                float tb = t0;
+                for (int k = 1; k < kPolicies; ++k) {
+                    if (!timed[k]) continue;
+                    put_lists(v1[k], vp[k]);
+                    const float t = time_run(2);
+                    if (t < 0.95f * t0 && t < tb) tb = t, best = k;
+                }
+                put_lists(v1[0], vp[0]);
+                if (short_rows && nA1 + nT1 > 0) {
+                    thread1[phase] = true;
+                    const float t = time_run(2);
+                    thread1[phase] = false;
+                    if (t < 0.95f * t0 && t < tb) tb = t, best = 0, thread = true;
+                }
+            }
             tuned[phase] = best;
+            thread1[phase] = thread;
             h1 = v1[best], hp = vp[best];
             put_lists(h1, hp);
             BK(cudaStreamSynchronize(s));
@@ -895,12 +927,14 @@ struct Batch final : BatchBase {
     // ------------------------------------------------------------------ launches
     template <class X, class E>
     void spmv_A(const X* xin, const E& e, const int* act) {
-        if (nA1) k_rowblock_batch<T, X, E, true><<<nA1, kThreads, 0, s>>>(Aptr, Aidx, Aval, xin, A1_it, Ae1_it, act, e), ++launches;
+        if (nA1 && thread1[0]) k_rowthread_batch<T, X, E><<<nA1, kThreads, 0, s>>>(Aptr, Aidx, Aval, xin, A1_it, Ae1_it, act, e), ++launches;
+        else if (nA1) k_rowblock_batch<T, X, E, true><<<nA1, kThreads, 0, s>>>(Aptr, Aidx, Aval, xin, A1_it, Ae1_it, act, e), ++launches;
         if (nAp) k_pack_spmv<T, X, E><<<nAp, kThreads, 0, s>>>(Aptr, Aidx, Aval, xin, A_it, Ae_it, slot_inst, act, e), ++launches;
     }
     template <class X, class E>
     void spmv_T(const X* xin, const E& e, const int* act) {
-        if (nT1) k_rowblock_batch<T, X, E, true><<<nT1, kThreads, 0, s>>>(Tptr, Tidx, Tval, xin, T1_it, Te1_it, act, e), ++launches;
+        if (nT1 && thread1[1]) k_rowthread_batch<T, X, E><<<nT1, kThreads, 0, s>>>(Tptr, Tidx, Tval, xin, T1_it, Te1_it, act, e), ++launches;
+        else if (nT1) k_rowblock_batch<T, X, E, true><<<nT1, kThreads, 0, s>>>(Tptr, Tidx, Tval, xin, T1_it, Te1_it, act, e), ++launches;
         if (nTp) k_pack_spmv<T, X, E><<<nTp, kThreads, 0, s>>>(Tptr, Tidx, Tval, xin, T_it, Te_it, slot_inst, act, e), ++launches;
     }
     void products(const int* act) {

@@ -115,7 +115,8 @@ struct CudaError {
     } while (0)
 
 struct DevMat {
-    int rows = 0;
+    int rows = 0, maxrow = 0;  // maxrow: the longest row's nonzeros
+    bool per_thread = false;   // SpMV by k_rowthread (one thread per row) instead of the row blocks
     int64_t nnz = 0;
     int *ptr = nullptr, *idx = nullptr;
     int4* blk = nullptr;
@@ -171,6 +172,7 @@ struct Engine final : EngineBase {
         d.rows = a.rows, d.nnz = a.nnz;
         std::vector<int> p32(size_t(a.rows) + 1);
         for (int r = 0; r <= a.rows; ++r) p32[r] = int(a.ptr[r]);
+        for (int r = 0; r < a.rows; ++r) d.maxrow = std::max(d.maxrow, p32[r + 1] - p32[r]);
         std::vector<int4> blk = build_row_blocks(a.ptr, a.rows);
         d.nblk = int(blk.size());
         d.ptr = alloc<int>(p32.size()), d.idx = alloc<int>(size_t(a.nnz)), d.blk = alloc<int4>(blk.size());
@@ -206,6 +208,7 @@ struct Engine final : EngineBase {
         d.rows = a.rows, d.nnz = int64_t(a.idx.size());
         std::vector<int> p32(size_t(a.rows) + 1);
         for (int r = 0; r <= a.rows; ++r) p32[r] = int(a.ptr[r]);
+        for (int r = 0; r < a.rows; ++r) d.maxrow = std::max(d.maxrow, p32[r + 1] - p32[r]);
         std::vector<int4> blk = build_row_blocks(a.ptr.data(), a.rows);
         d.nblk = int(blk.size());
         d.ptr = alloc<int>(p32.size()), d.idx = alloc<int>(size_t(d.nnz)), d.blk = alloc<int4>(blk.size());
@@ -309,56 +312,94 @@ struct Engine final : EngineBase {
     }
 
     // ------------------------------------------------------------------ autotuner
-    // Row-split policy per matrix (FP32 contexts, matrices of at least 2^20 nonzeros), timed on the matrix itself
-    // (CUDA-event time of 10 SpMV launches after 3 warm-ups): 0 the hybrid rule (thread per row up to 48 nonzeros,
-    // warp per longer row), 1 thread per row in the kUniformCandidate blocks, 2 the balanced segmented sums
-    // (kSegmented) in every block, 3 the hybrid rule with 8-lane groups for rows up to 128 nonzeros (kMidGroups),
-    // 4 policies 1 and 3 together. A policy other than 0 is kept only if it is at least 5 % faster. FP64 contexts
-    // keep policy 0 (the parity pins' summation order); TARAL_TUNE=0 keeps it everywhere.
+    // Per matrix of at least 2^20 nonzeros, timed on the matrix itself (CUDA-event time of 10 launches of its PDHG
+    // phase, the SpMV with its fused step, after 3 warm-ups, 13 before the first candidate; a choice other than the
+    // default is kept only if it is at least 5 % faster). Candidates that cannot change the arithmetic (policies 1,
+    // 3, 4 when no row exceeds kShort) are not timed, so noise cannot pick them:
+    // 1. FP32 contexts: the row-split policy of the block list (kernels.cuh): 0 the hybrid rule (thread per row up to
+    //    48 nonzeros, warp per longer row), 1 thread per row in the kUniformCandidate blocks, 2 the balanced
+    //    segmented sums (kSegmented) in every block, 3 the hybrid rule with 8-lane groups for rows up to 128
+    //    nonzeros (kMidGroups), 4 policies 1 and 3 together. FP64 contexts keep policy 0 (the parity pins'
+    //    summation order).
+    // 2. Any precision, matrices whose rows all hold at most kShort nonzeros: k_rowthread instead of the block
+    //    kernel (bit-identical results under policy 0, so FP64 may use it too).
+    // TARAL_TUNE=0 keeps the defaults; TARAL_ROWSPLIT=0..4 and TARAL_ROWTHREAD=0|1 force a choice, untimed.
     void tune() {
-        if (sizeof(T) != sizeof(float)) return;
         if (const char* e = std::getenv("TARAL_TUNE"))
             if (std::atoi(e) == 0) return;
-        const int forced = forced_row_split();  // that policy for every matrix, untimed (tests, experiments)
+        const int forced = forced_row_split();
+        int forced_thread = -1;
+        if (const char* e = std::getenv("TARAL_ROWTHREAD")) forced_thread = std::atoi(e) != 0 ? 1 : 0;
         int which = 0;
         for (DevMat* d : {&A, &AT}) {
             const int slot = which++;
-            if (d->nblk == 0 || (forced < 0 && d->nnz < (int64_t(1) << 20))) continue;  // small: timings are noise
-            std::vector<int4> base(size_t(d->nblk));
-            CK(cudaMemcpyAsync(base.data(), d->blk, base.size() * sizeof(int4), cudaMemcpyDeviceToHost, st));
-            CK(cudaStreamSynchronize(st));
-            std::vector<std::vector<int4>> cand(kPolicies, base);
-            bool differs[kPolicies] = {true};
-            for (int k = 1; k < kPolicies; ++k) differs[k] = apply_row_split(cand[k], k);
-            const T* xin = d == &A ? pv : pw;  // scratch vectors of the right length (power iteration)
-            T* yout = d == &A ? pw : pu;
-            auto time_list = [&](const std::vector<int4>& list) {
-                CK(cudaMemcpyAsync(d->blk, list.data(), list.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
-                for (int r = 0; r < 3; ++r) spmv(*d, xin, yout);
+            if (d->nblk == 0) continue;
+            const bool small = d->nnz < (int64_t(1) << 20);  // timings are noise
+            const bool short_rows = d->maxrow <= kShort;      // every row on the thread path of policy 0
+            // the phase itself with its fused step, on the not yet started state (start() rewrites every vector the
+            // steps write: x, xs, z, zs, Ax, ATz)
+            auto phase = [&] {
+                if (d == &A) rowblock(A, x, EpiRow<T>{Ax, z, zs, rl, ru, par});
+                else rowblock(AT, z, EpiCol<T>{ATz, x, xs, c, l, u, par, 1});
+            };
+            auto time_spmv = [&](int warm) {
+                for (int r = 0; r < warm; ++r) phase();
                 cudaEvent_t e0, e1;
                 CK(cudaEventCreate(&e0));
                 CK(cudaEventCreate(&e1));
                 CK(cudaEventRecord(e0, st));
-                for (int r = 0; r < 10; ++r) spmv(*d, xin, yout);
+                for (int r = 0; r < 10; ++r) phase();
                 CK(cudaEventRecord(e1, st));
                 CK(cudaEventSynchronize(e1));
                 float ms = 0;
                 CK(cudaEventElapsedTime(&ms, e0, e1));
                 cudaEventDestroy(e0), cudaEventDestroy(e1);
-                launches -= 13;  // tuning launches are not part of the solve's count
+                launches -= warm + 10;  // tuning launches are not part of the solve's count
                 return ms;
             };
+            std::vector<int4> base(size_t(d->nblk));
+            CK(cudaMemcpyAsync(base.data(), d->blk, base.size() * sizeof(int4), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            std::vector<std::vector<int4>> cand(kPolicies, base);
+            bool timed[kPolicies] = {true};
+            for (int k = 1; k < kPolicies; ++k) {
+                // FP32 only (FP64 keeps the parity pins' order); with short rows only policy 2 sums differently
+                const bool differs = apply_row_split(cand[k], k);
+                timed[k] = sizeof(T) == sizeof(float) && differs && (!short_rows || k == 2);
+            }
+            auto put = [&](const std::vector<int4>& list) {
+                CK(cudaMemcpyAsync(d->blk, list.data(), list.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
+            };
             int best = 0;
-            if (forced >= 0) {
-                best = forced;
-            } else {
-                float t[kPolicies];
-                for (int k = 0; k < kPolicies; ++k) t[k] = differs[k] ? time_list(cand[k]) : 1e30f;
-                for (int k = 1; k < kPolicies; ++k)
-                    if (t[k] < 0.95f * t[0] && t[k] < t[best]) best = k;
+            bool thread = false;
+            float t_pol[kPolicies] = {0}, t_thread = 0;
+            if (forced >= 0 || forced_thread >= 0) {
+                if (sizeof(T) == sizeof(float) && forced >= 0) best = forced;
+                thread = short_rows && best == 0 && forced_thread == 1;
+            } else if (!small) {
+                const float t0 = t_pol[0] = time_spmv(13);  // the first timings of a context also warm the GPU up
+                float tb = t0;
+                for (int k = 1; k < kPolicies; ++k) {
+                    if (!timed[k]) continue;
+                    put(cand[k]);
+                    const float t = t_pol[k] = time_spmv(3);
+                    if (t < 0.95f * t0 && t < tb) tb = t, best = k;
+                }
+                put(base);
+                if (short_rows) {
+                    d->per_thread = true;
+                    const float t = t_thread = time_spmv(3);
+                    d->per_thread = false;
+                    if (t < 0.95f * t0 && t < tb) tb = t, best = 0, thread = true;
+                }
+                if (std::getenv("TARAL_TIMING"))
+                    std::fprintf(stderr, "taral: tune %s: policies %.1f %.1f %.1f %.1f %.1f, thread per row %.1f us/launch\n",
+                                 slot ? "A^T" : "A", t_pol[0] * 100, t_pol[1] * 100, t_pol[2] * 100, t_pol[3] * 100,
+                                 t_pol[4] * 100, t_thread * 100);
             }
             tuned[slot] = best;
-            CK(cudaMemcpyAsync(d->blk, cand[best].data(), cand[best].size() * sizeof(int4), cudaMemcpyHostToDevice, st));
+            put(cand[best]);
+            d->per_thread = per_thread[slot] = thread;
             CK(cudaStreamSynchronize(st));
         }
     }
@@ -367,8 +408,12 @@ struct Engine final : EngineBase {
     template <class X, class E>
     void rowblock(const DevMat& a, const X* xin, const E& epi, const int* skip = nullptr) {
         if (a.nblk == 0) return;
-        k_rowblock<T, X, E, true><<<a.nblk, kThreads, 0, st>>>(a.ptr, a.idx, static_cast<const T*>(a.val), xin,
-                                                                a.blk, skip, epi);
+        if (a.per_thread)
+            k_rowthread<T, X, E><<<(a.rows + kThreads - 1) / kThreads, kThreads, 0, st>>>(
+                a.rows, a.ptr, a.idx, static_cast<const T*>(a.val), xin, skip, epi);
+        else
+            k_rowblock<T, X, E, true><<<a.nblk, kThreads, 0, st>>>(a.ptr, a.idx, static_cast<const T*>(a.val), xin,
+                                                                    a.blk, skip, epi);
         ++launches;
     }
     template <class X, class Y>

@@ -17,7 +17,8 @@ struct EngineBase {
     size_t mem_used = 0;
     int64_t launches = 0;
     int64_t nnz = 0;  // nonzeros of A
-    int tuned[2] = {0, 0};  // row-split policy chosen by the autotuner for A and A^T (1: thread per row)
+    int tuned[2] = {0, 0};  // row-split policy chosen by the autotuner for A and A^T
+    bool per_thread[2] = {false, false};  // A, A^T use the one-thread-per-row SpMV kernel
     virtual ~EngineBase() = default;
     virtual double power_norm(int iters) = 0;
     virtual void set_steps(double tau, double sigma) = 0;

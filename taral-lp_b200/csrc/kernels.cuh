@@ -59,6 +59,10 @@ __device__ __forceinline__ double gather(const double* p) {
     return v;
 }
 
+// Products rounded on their own (never fused into a following add), as the staged paths round them.
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+
 // Product type staged in shared memory: float products for a float matrix, double otherwise.
 template <class T, class X> struct ProdT { using type = double; };
 template <> struct ProdT<float, float> { using type = float; };
@@ -409,6 +413,26 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_rowblock(const int* __
     if (mine) epi.apply(r0 + tid, sm.rowsum[tid], ops);
 }
 
+// One thread per row, its products summed in entry order: for a matrix whose rows all hold at most kShort nonzeros
+// this is exactly block_sums' thread-per-row arithmetic (each product rounded to the product type, FP64 sums in
+// entry order), so the results are bit-identical; it skips the staging, the metadata and the block barriers, which
+// pays for very short rows (Engine::tune times both). `skip` as in k_rowblock.
+template <class T, class X, class E>
+__global__ void __launch_bounds__(kThreads) k_rowthread(int rows, const int* __restrict__ ptr,
+                                                        const int* __restrict__ idx, const T* __restrict__ val,
+                                                        const X* __restrict__ xin, const int* __restrict__ skip,
+                                                        E epi) {
+    using P = typename ProdT<T, X>::type;
+    if (skip && *skip) return;
+    const int r = blockIdx.x * kThreads + threadIdx.x;
+    if (r >= rows) return;
+    const typename E::Ops ops = epi.load(r, 0);
+    const int a = __ldg(ptr + r), b = __ldg(ptr + r + 1);
+    double s = 0;
+    for (int k = a; k < b; ++k) s += double(mul_rn(P(__ldg(val + k)), P(gather(xin + __ldg(idx + k)))));
+    epi.apply(r, s, ops);
+}
+
 // Batched form: a block list over many instances (block-diagonal batch). ext[b] = {instance, row shift, gather
 // offset, 0}: the block's rows r of the (possibly shared) matrix are rows r + shift of the concatenated instance
 // vectors, and its column indices address xin + offset. Blocks of instances with active[instance] == 0 return.
@@ -430,6 +454,30 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_rowblock_batch(const i
     if (mine) ops = epi.load(r0 + tid, e4.x);
     block_sums<T, X, VEC>(ptr, idx, val, xin + e4.z, meta, sm);
     if (mine) epi.apply(r0 + tid, sm.rowsum[tid], ops);
+}
+
+// Batched thread-per-row form over the same block lists as k_rowblock_batch: thread t of a CTA takes row t of the
+// block (threads past the block's rows return). Bit-identical to k_rowblock_batch under policy 0 when every row of
+// the matrix holds at most kShort nonzeros, for the reasons given at k_rowthread.
+template <class T, class X, class E>
+__global__ void __launch_bounds__(kThreads) k_rowthread_batch(const int* __restrict__ ptr, const int* __restrict__ idx,
+                                                              const T* __restrict__ val, const X* __restrict__ xin,
+                                                              const int4* __restrict__ blk,
+                                                              const int4* __restrict__ ext,
+                                                              const int* __restrict__ active, E epi) {
+    using P = typename ProdT<T, X>::type;
+    const int4 e4 = __ldg(ext + blockIdx.x);
+    if (!active[e4.x]) return;
+    const int4 meta = __ldg(blk + blockIdx.x);
+    const int t = threadIdx.x;
+    if (t >= (meta.y & 0xffff)) return;
+    const int r = meta.x + t;  // row of the shared matrix; row r + e4.y of the batch's vectors
+    const typename E::Ops ops = epi.load(r + e4.y, e4.x);
+    const int a = __ldg(ptr + r), b = __ldg(ptr + r + 1);
+    const X* xb = xin + e4.z;
+    double s = 0;
+    for (int k = a; k < b; ++k) s += double(mul_rn(P(__ldg(val + k)), P(gather(xb + __ldg(idx + k)))));
+    epi.apply(r + e4.y, s, ops);
 }
 
 // First primal step of a block (gpu/pdhg.cu:208-214): x = clamp(x - tau (c + ATz), l, u), xs += x.

@@ -109,7 +109,7 @@ int solve_model(const taral_model& md, const Options& o, SolveResult& res, const
     res.solve_s = since(t);
     res.kernel_launches = e->launches;
     res.nnz = e->nnz;
-    const int tuned_a = e->tuned[0], tuned_t = e->tuned[1];
+    const int tuned_a = e->tuned[0] + (e->per_thread[0] ? 10 : 0), tuned_t = e->tuned[1] + (e->per_thread[1] ? 10 : 0);
     t = Clock::now();
     res.fin = finish_point(md, P, res.outcome);
     const double finish_s = since(t);
@@ -118,7 +118,7 @@ int solve_model(const taral_model& md, const Options& o, SolveResult& res, const
     const double release_s = since(t);
     if (std::getenv("TARAL_TIMING"))
         std::fprintf(stderr, "taral: scale %.4f s, transfer %.4f s, solve %.4f s, finish %.4f s, release %.4f s, "
-                     "row-split policy A %d A^T %d\n", res.scale_s, res.transfer_s, res.solve_s, finish_s, release_s,
+                     "row-split policy A %d A^T %d (10: thread per row)\n", res.scale_s, res.transfer_s, res.solve_s, finish_s, release_s,
                      tuned_a, tuned_t);
     res.m = P.m, res.n = P.n;
     return TARAL_OK;

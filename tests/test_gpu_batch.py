@@ -121,3 +121,22 @@ def test_batch_tail_compaction_changes_nothing(engine_lib, monkeypatch, pack):
     for ya, yc in zip(y1, y3):
         assert np.array_equal(ya, yc)
     assert all(r["status"] == "near_optimal" for r in r1)
+
+
+@pytest.mark.parametrize("precision", [pdhg.FP64, pdhg.FP32])
+def test_batch_row_thread_kernel_is_bit_identical(engine_lib, monkeypatch, precision):
+    """The batched one-thread-per-row kernel (phases whose rows all hold at most 48 nonzeros: here A^T of the
+    refinery scenarios and both matrices of the packing LPs) gives the same counts and bit-identical points."""
+    base = lpgen.RefineryBase(3, seed=3)
+    pert = lpgen.perturbations(6, seed=9)
+    lps = [base.instance(2 + k % 2, pert[k]) for k in range(6)] + [lpgen.packing(1500, seed=k) for k in range(2)]
+    outs = []
+    for flag in ("0", "1"):
+        monkeypatch.setenv("TARAL_ROWTHREAD", flag)
+        b = pdhg.Batch(lps, tol=1e-6, precision=precision, time_limit=300)
+        outs.append(b.solve())
+    (r0, x0, y0), (r1, x1, y1) = outs
+    assert [r["iterations"] for r in r0] == [r["iterations"] for r in r1]
+    assert [r["objective"] for r in r0] == [r["objective"] for r in r1]
+    assert all(np.array_equal(a, c) for a, c in zip(x0, x1)) and all(np.array_equal(a, c) for a, c in zip(y0, y1))
+    assert all(r["status"] == "near_optimal" for r in r0)

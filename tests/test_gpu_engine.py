@@ -157,3 +157,19 @@ def test_row_split_policies_agree(engine_lib, monkeypatch, policy):
     r, x, _ = pdhg.solve(lp, tol=1e-6, precision=pdhg.FP32, time_limit=120)
     assert r["status"] == "near_optimal", r
     assert rel(r["objective"], lp.obj_star) < 1e-5, (r["objective"], lp.obj_star)
+
+
+@pytest.mark.parametrize("precision", [pdhg.FP64, pdhg.FP32])
+def test_row_thread_kernel_is_bit_identical(engine_lib, monkeypatch, precision):
+    # matrices whose rows all hold at most 48 nonzeros may run on the one-thread-per-row kernel: the same products
+    # summed in the same order as the row blocks' thread path, so the whole solve is bit-identical either way
+    lp = lpgen.packing(2000, seed=3)  # rows of A ~10, of A^T 5 nonzeros
+    outs = []
+    for flag in ("0", "1"):
+        monkeypatch.setenv("TARAL_ROWTHREAD", flag)
+        r, x, y = pdhg.solve(lp, tol=1e-6, precision=precision)
+        outs.append((r, x, y))
+    (r0, x0, y0), (r1, x1, y1) = outs
+    assert r0["status"] == r1["status"] == "near_optimal"
+    assert (r0["iterations"], r0["restarts"], r0["objective"]) == (r1["iterations"], r1["restarts"], r1["objective"])
+    assert np.array_equal(x0, x1) and np.array_equal(y0, y1)
