@@ -384,7 +384,7 @@ def our_arm(args, rank, world, dist):
             "e2e": {"value": e2e_value, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "phases_s": {k: e2e_out[-1][k] for k in ("scale_s", "device_init_s", "transfer_s", "solve_s")},
                     "steps_s": e2e_steps, "warmup_calls": 1},
-            "roofline": {"bound": "hbm", "kernel": f"{dom}-phase SpMV + fused step (k_rowblock)",
+            "roofline": {"bound": "hbm", "kernel": f"{dom}-phase SpMV + fused step (" + ("k_rowblock" if dom == "row" else "k_rowthread or k_rowblock, the tuner's choice") + ")",
                          "achieved": row_gbs if dom == "row" else col_gbs, "peak": peak, "unit": "GB/s",
                          "frac": (row_gbs if dom == "row" else col_gbs) / peak, "peak_kind": peak_kind,
                          "traffic": traffic, "row_ms": row_ms, "col_ms": col_ms,
