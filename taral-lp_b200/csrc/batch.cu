@@ -526,6 +526,10 @@ struct Batch final : BatchBase {
     T *Aval = nullptr, *Tval = nullptr;
     int4 *A_it = nullptr, *Ae_it = nullptr, *T_it = nullptr, *Te_it = nullptr;
     int4 *A1_it = nullptr, *Ae1_it = nullptr, *T1_it = nullptr, *Te1_it = nullptr;
+    // row-chunk lists of the width-1 packs for k_rowthread_batch: one warp per kChunk rows of one instance
+    int nA1r = 0, nT1r = 0;
+    int4 *A1_rc = nullptr, *Ae1_rc = nullptr, *T1_rc = nullptr, *Te1_rc = nullptr;
+    std::vector<int4> h_a1r, h_ae1r, h_t1r, h_te1r, c_a1r, c_ae1r, c_t1r, c_te1r;
     std::vector<int4> h_a1, h_ap, h_t1, h_tp;  // host copies of the iteration block lists (autotuner)
     std::vector<int4> h_ae1, h_ae, h_te1, h_te;  // and of their extensions (instance or pack of each entry)
     std::vector<int4> c_a1, c_ae1, c_ap, c_ae, c_t1, c_te1, c_tp, c_te;  // the compacted lists last uploaded
@@ -788,6 +792,22 @@ struct Batch final : BatchBase {
                     }
             }
         }
+        // row-chunk lists of the width-1 packs, in the same matrix-major order (a chunk, then its instances)
+        for (int k = 0; k < distinct; ++k) {
+            const Shared& sh = *mats[k];
+            for (int r0 = 0; r0 < sh.S.m; r0 += kChunk)
+                for (int p : packs_of[k])
+                    if (packs[p].W == 1)
+                        h_a1r.push_back(make_int4(sh.pbaseA + r0, std::min(kChunk, sh.S.m - r0), 0, 0)),
+                            h_ae1r.push_back(make_int4(packs[p].inst[0], packs[p].rbase - sh.pbaseA, packs[p].cbase, 0));
+            for (int r0 = 0; r0 < sh.S.n; r0 += kChunk)
+                for (int p : packs_of[k])
+                    if (packs[p].W == 1)
+                        h_t1r.push_back(make_int4(sh.pbaseT + r0, std::min(kChunk, sh.S.n - r0), 0, 0)),
+                            h_te1r.push_back(make_int4(packs[p].inst[0], packs[p].cbase - sh.pbaseT, packs[p].rbase, 0));
+        }
+        nA1r = int(h_a1r.size()), nT1r = int(h_t1r.size());
+        A1_rc = put(h_a1r), Ae1_rc = put(h_ae1r), T1_rc = put(h_t1r), Te1_rc = put(h_te1r);
         nA = int(a_ev.size()), nT = int(t_ev.size());
         nA1 = int(a1_it.size()), nT1 = int(t1_it.size()), nAp = int(a_it.size()), nTp = int(t_it.size());
         A1_it = put(a1_it), Ae1_it = put(ae1_it), T1_it = put(t1_it), Te1_it = put(te1_it);
@@ -835,8 +855,8 @@ struct Batch final : BatchBase {
     // its fused step (5 launches after 2 warm-ups, on the not yet started state: solve() rewrites every vector the
     // steps write); a choice other than the default is kept only if it is at least 5 % faster:
     // 1. FP32 batches: the engine's five row-split policies (policies 1, 3, 4 only where some row exceeds kShort);
-    // 2. any precision, phases whose matrices have no row over kShort nonzeros: k_rowthread_batch for the width-1
-    //    lists (bit-identical under policy 0).
+    // 2. k_rowthread_batch for the width-1 lists: any precision where no row exceeds kShort (bit-identical under
+    //    policy 0), FP32 also for rows up to kMid (every row by its own thread, entry order).
     // TARAL_TUNE=0 keeps the defaults; TARAL_ROWSPLIT=0..4 and TARAL_ROWTHREAD=0|1 force a choice, untimed.
     void tune() {
         if (const char* e = std::getenv("TARAL_TUNE"))
@@ -862,6 +882,7 @@ struct Batch final : BatchBase {
             int maxrow = 0;
             for (const auto& m : mats) maxrow = std::max(maxrow, phase ? m->maxrowT : m->maxrowA);
             const bool short_rows = maxrow <= kShort;
+            const bool thread_ok = short_rows || (sizeof(T) == sizeof(float) && maxrow <= kMid);
             auto put_lists = [&](const std::vector<int4>& l1, const std::vector<int4>& lp) {
                 if (!l1.empty()) BK(cudaMemcpyAsync(d1, l1.data(), l1.size() * sizeof(int4), cudaMemcpyHostToDevice, s));
                 if (!lp.empty()) BK(cudaMemcpyAsync(dp, lp.data(), lp.size() * sizeof(int4), cudaMemcpyHostToDevice, s));
@@ -895,7 +916,7 @@ struct Batch final : BatchBase {
             bool thread = false;
             if (!timing) {
                 if (sizeof(T) == sizeof(float) && forced >= 0) best = forced;
-                thread = short_rows && best == 0 && forced_thread == 1;
+                thread = thread_ok && best == 0 && forced_thread == 1;
             } else {
                 put_lists(v1[0], vp[0]);
                 const float t0 = time_run(6);
@@ -907,7 +928,7 @@ struct Batch final : BatchBase {
                     if (t < 0.95f * t0 && t < tb) tb = t, best = k;
                 }
                 put_lists(v1[0], vp[0]);
-                if (short_rows && nA1 + nT1 > 0) {
+                if (thread_ok && (phase ? nT1r : nA1r) > 0) {
                     thread1[phase] = true;
                     const float t = time_run(2);
                     thread1[phase] = false;
@@ -916,6 +937,9 @@ struct Batch final : BatchBase {
             }
             tuned[phase] = best;
             thread1[phase] = thread;
+            if (std::getenv("TARAL_TIMING"))
+                std::fprintf(stderr, "taral: batch tune %s: policy %d%s\n", phase ? "A^T" : "A", best,
+                             thread ? ", thread per row" : "");
             h1 = v1[best], hp = vp[best];
             put_lists(h1, hp);
             BK(cudaStreamSynchronize(s));
@@ -927,13 +951,13 @@ struct Batch final : BatchBase {
     // ------------------------------------------------------------------ launches
     template <class X, class E>
     void spmv_A(const X* xin, const E& e, const int* act) {
-        if (nA1 && thread1[0]) k_rowthread_batch<T, X, E><<<nA1, kThreads, 0, s>>>(Aptr, Aidx, Aval, xin, A1_it, Ae1_it, act, e), ++launches;
+        if (thread1[0] && nA1r) k_rowthread_batch<T, X, E><<<(nA1r + 7) / 8, kThreads, 0, s>>>(nA1r, Aptr, Aidx, Aval, xin, A1_rc, Ae1_rc, act, e), ++launches;
         else if (nA1) k_rowblock_batch<T, X, E, true><<<nA1, kThreads, 0, s>>>(Aptr, Aidx, Aval, xin, A1_it, Ae1_it, act, e), ++launches;
         if (nAp) k_pack_spmv<T, X, E><<<nAp, kThreads, 0, s>>>(Aptr, Aidx, Aval, xin, A_it, Ae_it, slot_inst, act, e), ++launches;
     }
     template <class X, class E>
     void spmv_T(const X* xin, const E& e, const int* act) {
-        if (nT1 && thread1[1]) k_rowthread_batch<T, X, E><<<nT1, kThreads, 0, s>>>(Tptr, Tidx, Tval, xin, T1_it, Te1_it, act, e), ++launches;
+        if (thread1[1] && nT1r) k_rowthread_batch<T, X, E><<<(nT1r + 7) / 8, kThreads, 0, s>>>(nT1r, Tptr, Tidx, Tval, xin, T1_rc, Te1_rc, act, e), ++launches;
         else if (nT1) k_rowblock_batch<T, X, E, true><<<nT1, kThreads, 0, s>>>(Tptr, Tidx, Tval, xin, T1_it, Te1_it, act, e), ++launches;
         if (nTp) k_pack_spmv<T, X, E><<<nTp, kThreads, 0, s>>>(Tptr, Tidx, Tval, xin, T_it, Te_it, slot_inst, act, e), ++launches;
     }
@@ -973,6 +997,14 @@ struct Batch final : BatchBase {
             graph = nullptr;
         }
     }
+    void upload_chunks(const std::vector<int4>& a, const std::vector<int4>& ae, const std::vector<int4>& t,
+                       const std::vector<int4>& te) {
+        auto up = [&](int4* d, const std::vector<int4>& h) {
+            if (!h.empty()) BK(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(int4), cudaMemcpyHostToDevice, s));
+        };
+        up(A1_rc, a), up(Ae1_rc, ae), up(T1_rc, t), up(Te1_rc, te);
+        nA1r = int(a.size()), nT1r = int(t.size());
+    }
     void compact_lists(const std::vector<int>& live) {
         auto pick = [&](const std::vector<int4>& blk, const std::vector<int4>& ext, bool one, std::vector<int4>& ob,
                         std::vector<int4>& oe) {
@@ -990,12 +1022,15 @@ struct Batch final : BatchBase {
         };
         pick(h_a1, h_ae1, true, c_a1, c_ae1), pick(h_ap, h_ae, false, c_ap, c_ae);
         pick(h_t1, h_te1, true, c_t1, c_te1), pick(h_tp, h_te, false, c_tp, c_te);
+        pick(h_a1r, h_ae1r, true, c_a1r, c_ae1r), pick(h_t1r, h_te1r, true, c_t1r, c_te1r);
         upload_lists(c_a1, c_ae1, c_ap, c_ae, c_t1, c_te1, c_tp, c_te);
+        upload_chunks(c_a1r, c_ae1r, c_t1r, c_te1r);
         compacted = true;
     }
     void restore_lists() {
         if (!compacted) return;
         upload_lists(h_a1, h_ae1, h_ap, h_ae, h_t1, h_te1, h_tp, h_te);
+        upload_chunks(h_a1r, h_ae1r, h_t1r, h_te1r);
         compacted = false;
     }
 

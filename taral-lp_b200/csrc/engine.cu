@@ -321,8 +321,9 @@ struct Engine final : EngineBase {
     //    segmented sums (kSegmented) in every block, 3 the hybrid rule with 8-lane groups for rows up to 128
     //    nonzeros (kMidGroups), 4 policies 1 and 3 together. FP64 contexts keep policy 0 (the parity pins'
     //    summation order).
-    // 2. Any precision, matrices whose rows all hold at most kShort nonzeros: k_rowthread instead of the block
-    //    kernel (bit-identical results under policy 0, so FP64 may use it too).
+    // 2. k_rowthread instead of the block kernel: in any precision for matrices whose rows all hold at most kShort
+    //    nonzeros (bit-identical results under policy 0, so FP64 may use it too); in FP32 also for rows up to kMid
+    //    (every row summed by its own thread in entry order).
     // TARAL_TUNE=0 keeps the defaults; TARAL_ROWSPLIT=0..4 and TARAL_ROWTHREAD=0|1 force a choice, untimed.
     void tune() {
         if (const char* e = std::getenv("TARAL_TUNE"))
@@ -336,6 +337,9 @@ struct Engine final : EngineBase {
             if (d->nblk == 0) continue;
             const bool small = d->nnz < (int64_t(1) << 20);  // timings are noise
             const bool short_rows = d->maxrow <= kShort;      // every row on the thread path of policy 0
+            // the thread-per-row kernel: bit-identical with short rows; otherwise (FP32, rows up to kMid) it sums
+            // every row by its own thread, as policy 1 does in uniform blocks
+            const bool thread_ok = short_rows || (sizeof(T) == sizeof(float) && d->maxrow <= kMid);
             // the phase itself with its fused step, on the not yet started state (start() rewrites every vector the
             // steps write: x, xs, z, zs, Ax, ATz)
             auto phase = [&] {
@@ -375,7 +379,7 @@ struct Engine final : EngineBase {
             float t_pol[kPolicies] = {0}, t_thread = 0;
             if (forced >= 0 || forced_thread >= 0) {
                 if (sizeof(T) == sizeof(float) && forced >= 0) best = forced;
-                thread = short_rows && best == 0 && forced_thread == 1;
+                thread = thread_ok && best == 0 && forced_thread == 1;
             } else if (!small) {
                 const float t0 = t_pol[0] = time_spmv(13);  // the first timings of a context also warm the GPU up
                 float tb = t0;
@@ -386,7 +390,7 @@ struct Engine final : EngineBase {
                     if (t < 0.95f * t0 && t < tb) tb = t, best = k;
                 }
                 put(base);
-                if (short_rows) {
+                if (thread_ok) {
                     d->per_thread = true;
                     const float t = t_thread = time_spmv(3);
                     d->per_thread = false;

@@ -456,22 +456,27 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_rowblock_batch(const i
     if (mine) epi.apply(r0 + tid, sm.rowsum[tid], ops);
 }
 
-// Batched thread-per-row form over the same block lists as k_rowblock_batch: thread t of a CTA takes row t of the
-// block (threads past the block's rows return). Bit-identical to k_rowblock_batch under policy 0 when every row of
-// the matrix holds at most kShort nonzeros, for the reasons given at k_rowthread.
+// Batched thread-per-row form: one warp per entry of a row-chunk list, chunk[e] = {first row in the concatenated
+// row pointers, rows (at most 32), -, -} of one instance, ext[e] = {instance, row shift, gather offset, 0} as for
+// k_rowblock_batch; lane t takes the chunk's row t. Bit-identical to k_rowblock_batch under policy 0 when every row
+// of the matrix holds at most kShort nonzeros, for the reasons given at k_rowthread.
+constexpr int kChunk = 32;  // rows per chunk: one warp
 template <class T, class X, class E>
-__global__ void __launch_bounds__(kThreads) k_rowthread_batch(const int* __restrict__ ptr, const int* __restrict__ idx,
-                                                              const T* __restrict__ val, const X* __restrict__ xin,
-                                                              const int4* __restrict__ blk,
+__global__ void __launch_bounds__(kThreads) k_rowthread_batch(int n, const int* __restrict__ ptr,
+                                                              const int* __restrict__ idx, const T* __restrict__ val,
+                                                              const X* __restrict__ xin,
+                                                              const int4* __restrict__ chunk,
                                                               const int4* __restrict__ ext,
                                                               const int* __restrict__ active, E epi) {
     using P = typename ProdT<T, X>::type;
-    const int4 e4 = __ldg(ext + blockIdx.x);
+    const int e = blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5);
+    if (e >= n) return;
+    const int4 e4 = __ldg(ext + e);
     if (!active[e4.x]) return;
-    const int4 meta = __ldg(blk + blockIdx.x);
-    const int t = threadIdx.x;
-    if (t >= (meta.y & 0xffff)) return;
-    const int r = meta.x + t;  // row of the shared matrix; row r + e4.y of the batch's vectors
+    const int4 c4 = __ldg(chunk + e);
+    const int t = threadIdx.x & 31;
+    if (t >= c4.y) return;
+    const int r = c4.x + t;  // row of the shared matrix; row r + e4.y of the batch's vectors
     const typename E::Ops ops = epi.load(r + e4.y, e4.x);
     const int a = __ldg(ptr + r), b = __ldg(ptr + r + 1);
     const X* xb = xin + e4.z;

@@ -125,11 +125,14 @@ def test_batch_tail_compaction_changes_nothing(engine_lib, monkeypatch, pack):
 
 @pytest.mark.parametrize("precision", [pdhg.FP64, pdhg.FP32])
 def test_batch_row_thread_kernel_is_bit_identical(engine_lib, monkeypatch, precision):
-    """The batched one-thread-per-row kernel (phases whose rows all hold at most 48 nonzeros: here A^T of the
-    refinery scenarios and both matrices of the packing LPs) gives the same counts and bit-identical points."""
-    base = lpgen.RefineryBase(3, seed=3)
-    pert = lpgen.perturbations(6, seed=9)
-    lps = [base.instance(2 + k % 2, pert[k]) for k in range(6)] + [lpgen.packing(1500, seed=k) for k in range(2)]
+    """The batched one-thread-per-row kernel (one warp per 32-row chunk of one scenario) on phases whose rows all hold
+    at most 48 nonzeros gives the same counts and bit-identical points: in FP64 the refinery scenarios' A^T and both
+    matrices of the packing LPs (their A, rows up to 112, stays on the row blocks); in FP32 the packing LPs."""
+    lps = [lpgen.packing(1500, seed=k) for k in range(3)]
+    if precision == pdhg.FP64:
+        base = lpgen.RefineryBase(3, seed=3)
+        pert = lpgen.perturbations(6, seed=9)
+        lps = [base.instance(2 + k % 2, pert[k]) for k in range(6)] + lps
     outs = []
     for flag in ("0", "1"):
         monkeypatch.setenv("TARAL_ROWTHREAD", flag)
@@ -140,3 +143,20 @@ def test_batch_row_thread_kernel_is_bit_identical(engine_lib, monkeypatch, preci
     assert [r["objective"] for r in r0] == [r["objective"] for r in r1]
     assert all(np.array_equal(a, c) for a, c in zip(x0, x1)) and all(np.array_equal(a, c) for a, c in zip(y0, y1))
     assert all(r["status"] == "near_optimal" for r in r0)
+
+
+def test_batch_row_thread_kernel_fp32_medium_rows(engine_lib, monkeypatch):
+    """In FP32 the thread-per-row kernel also takes rows of up to 128 nonzeros (the refinery A): every row summed by
+    one thread in entry order, a different order than the row blocks' warps, so the answers agree to the tolerance,
+    not bitwise."""
+    base = lpgen.RefineryBase(3, seed=3)
+    pert = lpgen.perturbations(6, seed=9)
+    lps = [base.instance(2 + k % 2, pert[k]) for k in range(6)]
+    outs = []
+    for flag in ("0", "1"):
+        monkeypatch.setenv("TARAL_ROWTHREAD", flag)
+        b = pdhg.Batch(lps, tol=1e-6, precision=pdhg.FP32, time_limit=300)
+        outs.append(b.solve()[0])
+    for a, c in zip(*outs):
+        assert a["status"] == c["status"] == "near_optimal"
+        assert rel(a["objective"], c["objective"]) < 5e-6, (a["objective"], c["objective"])
