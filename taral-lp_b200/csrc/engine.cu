@@ -806,6 +806,7 @@ extern "C" void pdhg_destroy(pdhg_ctx* ctx) { delete ctx; }
 // ================================================================================================ SpMV plan
 struct taral_spmv_plan {
     int rows = 0, cols = 0, dtype = TARAL_FP64, nblk = 0;
+    bool per_thread = false;  // every row holds at most kShort nonzeros: k_rowthread (bit-identical, no staging)
     int4* blk = nullptr;
 };
 
@@ -817,9 +818,14 @@ extern "C" int taral_spmv_plan_create(int rows, int cols, const int64_t* host_pt
         if (host_ptr[r + 1] < host_ptr[r]) return TARAL_ERR_INPUT;
     if (host_ptr[rows] > INT32_MAX - 64) return TARAL_ERR_INPUT;
     std::vector<int4> blk = taral::build_row_blocks(host_ptr, rows);
-    if (taral::forced_row_split() > 0) taral::apply_row_split(blk, taral::forced_row_split());  // tests
+    const int forced = taral::forced_row_split();  // tests
+    if (forced > 0) taral::apply_row_split(blk, forced);
+    int64_t maxrow = 0;
+    for (int r = 0; r < rows; ++r) maxrow = std::max<int64_t>(maxrow, host_ptr[r + 1] - host_ptr[r]);
+    const char* rt = std::getenv("TARAL_ROWTHREAD");
     auto* p = new taral_spmv_plan;
     p->rows = rows, p->cols = cols, p->dtype = dtype, p->nblk = int(blk.size());
+    p->per_thread = maxrow <= taral::kShort && forced <= 0 && !(rt && std::atoi(rt) == 0);
     if (cudaMalloc(&p->blk, std::max<size_t>(blk.size(), 1) * sizeof(int4)) != cudaSuccess) {
         delete p;
         return TARAL_ERR_ALLOC;
@@ -840,7 +846,10 @@ static void spmv_launch(const taral_spmv_plan* p, const int* ptr, const int* idx
     using namespace taral;
     bool vec = (reinterpret_cast<uintptr_t>(idx) % 16 == 0) && (reinterpret_cast<uintptr_t>(val) % 16 == 0);
     EpiStore<T> e{static_cast<T*>(y)};
-    if (vec)
+    if (p->per_thread)
+        k_rowthread<T, T, EpiStore<T>><<<(p->rows + kThreads - 1) / kThreads, kThreads, 0, s>>>(
+            p->rows, ptr, idx, static_cast<const T*>(val), static_cast<const T*>(x), nullptr, e);
+    else if (vec)
         k_rowblock<T, T, EpiStore<T>, true><<<p->nblk, kThreads, 0, s>>>(ptr, idx, static_cast<const T*>(val),
                                                                           static_cast<const T*>(x), p->blk, nullptr, e);
     else

@@ -3,8 +3,9 @@
 Every row-split policy of the autotuner (forced through TARAL_ROWSPLIT) sums the same products in a fixed order of
 its own, so in FP64 each row agrees with the oracle's sequential sum to rounding (bounded by n eps sum|a x|); in
 FP32 the products are rounded to float and summed in FP64, then the sum is rounded to float. Matrices cover rows
-longer than a block (the whole-CTA path), rows of 49..128 nonzeros (the 8-lane groups), empty rows, an empty matrix
-and index / value arrays that are not 16-byte aligned (the scalar staging path)."""
+longer than a block (the whole-CTA path), rows of 49..128 nonzeros (the 8-lane groups), empty rows, an empty matrix,
+index / value arrays that are not 16-byte aligned (the scalar staging path) and a matrix whose rows all hold at most
+48 nonzeros (one thread per row under policy 0, bit-identical to the staged kernel)."""
 import numpy as np
 import pytest
 
@@ -26,6 +27,10 @@ def _matrices():
     idx = np.concatenate([np.sort(rng.choice(5000, size=k, replace=False)) for k in lens]).astype(np.int32)
     val = rng.standard_normal(int(ptr[-1]))
     yield "mid_rows_and_empty", (ptr, idx, val)
+    lens = rng.integers(0, 49, size=5000)  # every row <= 48 nonzeros: the one-thread-per-row kernel
+    ptr = np.concatenate([[0], np.cumsum(lens)]).astype(np.int64)
+    idx = np.concatenate([np.sort(rng.choice(3000, size=k, replace=False)) for k in lens]).astype(np.int32)
+    yield "short_rows", (ptr, idx, rng.standard_normal(int(ptr[-1])))
 
 
 def _run(ptr, idx, val, x, dtype, offset=0):
@@ -81,3 +86,15 @@ def test_spmv_empty_and_bad_input(engine_lib):
     assert len(_run(np.zeros(1, np.int64), np.zeros(0, np.int32), np.zeros(0), np.ones(4), pdhg.FP64)) == 0
     with pytest.raises(pdhg.TaralError):
         pdhg.SpmvPlan(np.array([0, 3, 2], np.int64), 4, pdhg.FP64)  # decreasing row pointer
+
+
+@pytest.mark.parametrize("dtype", [pdhg.FP64, pdhg.FP32])
+def test_spmv_row_thread_is_bit_identical(engine_lib, monkeypatch, dtype):
+    ptr, idx, val = list(_matrices())[-1][1]
+    x = np.random.default_rng(2).standard_normal(int(idx.max()) + 1)
+    if dtype == pdhg.FP32:
+        val, x = val.astype(np.float32), x.astype(np.float32)
+    y_thread = _run(ptr, idx, val, x, dtype)
+    monkeypatch.setenv("TARAL_ROWTHREAD", "0")
+    y_staged = _run(ptr, idx, val, x, dtype)
+    assert np.array_equal(y_thread, y_staged)
