@@ -117,6 +117,7 @@ struct CudaError {
 struct DevMat {
     int rows = 0, maxrow = 0;  // maxrow: the longest row's nonzeros
     bool per_thread = false;   // SpMV by k_rowthread (one thread per row) instead of the row blocks
+    int split = 0;             // rows [0, split) by k_rowthread, the row blocks cover [split, rows)
     int64_t nnz = 0;
     int *ptr = nullptr, *idx = nullptr;
     int4* blk = nullptr;
@@ -202,14 +203,64 @@ struct Engine final : EngineBase {
         nnz = hA.nnz;
         finish_init(hc_ptr, hl, hu, hrl_ptr, hru_ptr, hDr, hDc);
     }
+    // Internal row order (FP32 contexts built from a model whose rows are of both kinds, short (<= kShort nonzeros)
+    // and long): rows sorted by ascending length (stable). The row phase's blocks then hold rows of similar length,
+    // and the column phase's gathers of z concentrate on a contiguous tail (a long row of A is gathered by many
+    // columns), which L1 and L2 serve far better. Every row's entries keep their order and A^T's entries keep
+    // theirs (renumbered), so both phases add the same products in the same order as in the model's row order;
+    // only the FP64 KKT sums over rows change order. TARAL_ROWORDER=0 keeps the model's order; 2 also runs the
+    // short prefix on the thread-per-row kernel (measured slower). rperm[k] = model row at position k.
+    std::vector<int> rperm;
+    int rsplit = 0;
+    bool order_rows(const Csr& a, const Csr& at, Csr& ap, Csr& atp) {
+        rperm.clear(), rsplit = 0;
+        const char* e = std::getenv("TARAL_ROWORDER");  // 0 off, 1 (default) sorted rows, 2 plus the thread prefix
+        const int mode = e ? std::atoi(e) : 1;
+        if (sizeof(T) != sizeof(float) || mode <= 0 || a.rows == 0) return false;
+        const int rows = a.rows;
+        std::vector<int> perm(static_cast<size_t>(rows));
+        for (int r = 0; r < rows; ++r) perm[size_t(r)] = r;
+        auto len = [&](int r) { return a.ptr[size_t(r) + 1] - a.ptr[size_t(r)]; };
+        std::stable_sort(perm.begin(), perm.end(), [&](int x, int y) { return len(x) < len(y); });
+        int split = 0;
+        while (split < rows && len(perm[size_t(split)]) <= kShort) ++split;
+        if (split == rows || split == 0) return false;  // rows of one kind: nothing to separate
+        std::vector<int> inv(static_cast<size_t>(rows));
+        for (int k = 0; k < rows; ++k) inv[size_t(perm[size_t(k)])] = k;
+        ap.rows = rows;
+        ap.ptr.assign(size_t(rows) + 1, 0);
+        ap.idx.resize(a.idx.size()), ap.val.resize(a.val.size());
+        for (int k = 0; k < rows; ++k) {
+            const int64_t b = a.ptr[size_t(perm[size_t(k)])], l = len(perm[size_t(k)]), o = ap.ptr[size_t(k)];
+            std::copy(a.idx.begin() + b, a.idx.begin() + b + l, ap.idx.begin() + o);
+            std::copy(a.val.begin() + b, a.val.begin() + b + l, ap.val.begin() + o);
+            ap.ptr[size_t(k) + 1] = o + l;
+        }
+        atp.rows = at.rows, atp.ptr = at.ptr, atp.val = at.val;
+        atp.idx.resize(at.idx.size());
+        for (size_t q = 0; q < at.idx.size(); ++q) atp.idx[q] = inv[size_t(at.idx[q])];
+        rperm = std::move(perm), rsplit = mode == 2 ? split : 0;
+        return true;
+    }
+    std::vector<double> to_internal(const std::vector<double>& v) const {  // model row order -> internal
+        std::vector<double> o(v.size());
+        for (size_t k = 0; k < v.size(); ++k) o[k] = v[size_t(rperm[k])];
+        return o;
+    }
+    std::vector<double> to_model(const std::vector<double>& v) const {  // internal -> model row order
+        std::vector<double> o(v.size());
+        for (size_t k = 0; k < v.size(); ++k) o[size_t(rperm[k])] = v[k];
+        return o;
+    }
     // Row pointers, column indices and row blocks of one matrix on the device; the values are left to the caller.
-    DevMat upload_structure(const Csr& a) {
+    DevMat upload_structure(const Csr& a, int split = 0) {
         DevMat d;
-        d.rows = a.rows, d.nnz = int64_t(a.idx.size());
+        d.rows = a.rows, d.nnz = int64_t(a.idx.size()), d.split = split;
         std::vector<int> p32(size_t(a.rows) + 1);
         for (int r = 0; r <= a.rows; ++r) p32[r] = int(a.ptr[r]);
         for (int r = 0; r < a.rows; ++r) d.maxrow = std::max(d.maxrow, p32[r + 1] - p32[r]);
-        std::vector<int4> blk = build_row_blocks(a.ptr.data(), a.rows);
+        std::vector<int4> blk = build_row_blocks(a.ptr.data() + split, a.rows - split);
+        for (int4& b : blk) b.x += split;  // rows counted from the split
         d.nblk = int(blk.size());
         d.ptr = alloc<int>(p32.size()), d.idx = alloc<int>(size_t(d.nnz)), d.blk = alloc<int4>(blk.size());
         CK(cudaMemcpyAsync(d.ptr, p32.data(), p32.size() * sizeof(int), cudaMemcpyHostToDevice, st));
@@ -228,9 +279,15 @@ struct Engine final : EngineBase {
         auto t0 = Clock::now();
         Csr hA, hAT;
         model_matrices(md, hA, hAT);
+        // FP32: rows in ascending length internally (rperm: internal -> model row); A^T keeps its entry order (its
+        // indices renumbered), so both phases sum exactly as before
+        Csr hAp, hATp;
+        const bool reorder = order_rows(hA, hAT, hAp, hATp);
+        const Csr& uA = reorder ? hAp : hA;
+        const Csr& uAT = reorder ? hATp : hAT;
         double hs = since(t0);
         begin(md.m, md.n, freq, flags);
-        A = upload_structure(hA), AT = upload_structure(hAT);
+        A = upload_structure(uA, reorder ? rsplit : 0), AT = upload_structure(uAT);
         const int64_t nz = int64_t(hA.val.size());
         P.m = m, P.n = n;
         P.Dr.resize(size_t(m)), P.Dc.resize(size_t(n));
@@ -254,8 +311,8 @@ struct Engine final : EngineBase {
         }
         dr = scratch(size_t(m)), dc = scratch(size_t(n)), rs = scratch(size_t(m)), cs = scratch(size_t(n));
         if (nz) {
-            CK(cudaMemcpyAsync(va, hA.val.data(), size_t(nz) * sizeof(double), cudaMemcpyHostToDevice, st));
-            CK(cudaMemcpyAsync(vt, hAT.val.data(), size_t(nz) * sizeof(double), cudaMemcpyHostToDevice, st));
+            CK(cudaMemcpyAsync(va, uA.val.data(), size_t(nz) * sizeof(double), cudaMemcpyHostToDevice, st));
+            CK(cudaMemcpyAsync(vt, uAT.val.data(), size_t(nz) * sizeof(double), cudaMemcpyHostToDevice, st));
         }
         scale_on_device(m, n, A.ptr, A.idx, va, AT.ptr, AT.idx, vt, dr, dc, rs, cs, st);
         if (sizeof(T) != sizeof(double) && nz) {
@@ -269,13 +326,21 @@ struct Engine final : EngineBase {
         CK(cudaGetLastError());
         }  // FP64 scratch released
         t0 = Clock::now();
+        if (reorder) P.Dr = to_model(P.Dr);
+        hAp = Csr(), hATp = Csr();
         P.A = std::move(hA), P.AT = Csr();  // the unscaled row-wise copy serves the original-space check
         P.a_original = true;
         hAT = Csr();
         scale_vectors(md, sign, P.Dr, P.Dc, P);
         hs += since(t0);
         if (host_s) *host_s = hs;
-        finish_init(P.c.data(), P.l.data(), P.u.data(), P.rl.data(), P.ru.data(), P.Dr.data(), P.Dc.data());
+        if (reorder) {
+            const std::vector<double> rl_i = to_internal(P.rl), ru_i = to_internal(P.ru), dr_i = to_internal(P.Dr);
+            finish_init(P.c.data(), P.l.data(), P.u.data(), rl_i.data(), ru_i.data(), dr_i.data(), P.Dc.data());
+            hrl = P.rl, hru = P.ru;  // the driver's host copies stay in the model's order
+        } else {
+            finish_init(P.c.data(), P.l.data(), P.u.data(), P.rl.data(), P.ru.data(), P.Dr.data(), P.Dc.data());
+        }
         nnz = nz;
     }
     void finish_init(const double* hc_ptr, const double* hl, const double* hu, const double* hrl_ptr,
@@ -411,6 +476,11 @@ struct Engine final : EngineBase {
     // ------------------------------------------------------------------ SpMV-shaped launches
     template <class X, class E>
     void rowblock(const DevMat& a, const X* xin, const E& epi, const int* skip = nullptr) {
+        if (a.split > 0) {  // the short-row prefix of a length-ordered matrix
+            k_rowthread<T, X, E><<<(a.split + kThreads - 1) / kThreads, kThreads, 0, st>>>(
+                a.split, a.ptr, a.idx, static_cast<const T*>(a.val), xin, skip, epi);
+            ++launches;
+        }
         if (a.nblk == 0) return;
         if (a.per_thread)
             k_rowthread<T, X, E><<<(a.rows + kThreads - 1) / kThreads, kThreads, 0, st>>>(
@@ -476,6 +546,8 @@ struct Engine final : EngineBase {
             k_start_x<T><<<grid_for(n), 256, 0, st>>>(n, l, u, x, xlast, xs);
         }
         ++launches;
+        std::vector<double> z0_i;
+        if (z0 && !rperm.empty()) z0_i = to_internal(std::vector<double>(z0, z0 + m)), z0 = z0_i.data();
         if (z0) {  // the copy into d_in above has been consumed in stream order before this one lands
             CK(cudaMemcpyAsync(d_in, z0, size_t(m) * sizeof(double), cudaMemcpyHostToDevice, st));
             k_set_point<T><<<grid_for(m), 256, 0, st>>>(m, d_in, z, zlast, zs);
@@ -566,6 +638,10 @@ struct Engine final : EngineBase {
             else k_scale_out<T><<<grid_for(m), 256, 0, st>>>(m, 1.0, z, hbuf);
             CK(cudaMemcpyAsync(hz, hbuf, size_t(m) * sizeof(double), cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));
+            if (!rperm.empty()) {
+                const std::vector<double> zm = to_model(std::vector<double>(hz, hz + m));
+                std::copy(zm.begin(), zm.end(), hz);
+            }
         }
         launches += 2;
         CK(cudaGetLastError());
