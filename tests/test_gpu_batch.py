@@ -85,6 +85,7 @@ def test_batch_packs_match_single_solves(engine_lib, monkeypatch, width):
     # unused slot, a pack of 2. Each batched instance takes the iterates of the same LP solved alone.
     monkeypatch.setenv("TARAL_BATCH_PACK", width)
     monkeypatch.setenv("TARAL_TUNE", "0")  # both sides on the default row split, whatever their timings
+    monkeypatch.setenv("TARAL_ROWORDER", "0")  # and the single solves in the model's row order, like the batch
     base = lpgen.RefineryBase(2, seed=5)
     pert = lpgen.perturbations(13, seed=8)
     lps = [base.instance(2, p) for p in pert[:11]] + [base.instance(1, p) for p in pert[11:]]
