@@ -216,6 +216,102 @@ bool tokenize_columns(const std::string& buf, size_t b, size_t e, int threads, c
     return true;
 }
 
+// The offset where the section starting at pos ends: the next section header line, or the end of the buffer.
+size_t section_end(const std::string& buf, size_t pos) {
+    size_t end = pos;
+    while (end < buf.size()) {
+        size_t nl = buf.find('\n', end);
+        if (nl == std::string::npos) nl = buf.size();
+        std::string_view l(buf.data() + end, nl - end);
+        if (!l.empty() && l.back() == '\r') l.remove_suffix(1);
+        if (is_header(l)) break;
+        end = nl + 1;
+    }
+    return std::min(end, buf.size());
+}
+
+// One line of the BOUNDS section, tokenised: the bound set named on the line (may be empty), the column, the
+// bound type (index into kBoundTypes) and value, or the line's error: `early` errors (a malformed line) come before
+// the bound-set test, the others (unknown column, bad number, unsupported type) after it, as in the sequential pass.
+constexpr std::string_view kBoundTypes[] = {"LO", "UP", "FX", "FR", "MI", "PL", "BV", "LI", "UI"};
+struct BoundRec {
+    std::string_view set;
+    int col = -1, type = -1, err = -1;  // err: index into the chunk's messages, -1 if none
+    bool early = false;
+    double v = 0;
+};
+
+// Tokenise the free-format BOUNDS lines in [b, e) of buf on `threads` threads (line-aligned chunks, records and
+// error messages per chunk, in file order). Column names are looked up in col_of (read only).
+template <class ColOf>
+void tokenize_bounds(const std::string& buf, size_t b, size_t e, int threads, const ColOf& col_of,
+                     std::vector<std::vector<BoundRec>>& parts, std::vector<std::vector<std::string>>& errs) {
+    std::vector<size_t> cut{b};
+    for (int q = 1; q < threads; ++q) {
+        size_t p = std::max(b + (e - b) * size_t(q) / size_t(threads), cut.back());
+        const size_t nl = buf.find('\n', p);
+        cut.push_back(nl == std::string::npos || nl >= e ? e : nl + 1);
+    }
+    cut.push_back(e);
+    const size_t nparts = static_cast<size_t>(threads);
+    parts.assign(nparts, std::vector<BoundRec>());
+    errs.assign(nparts, std::vector<std::string>());
+    auto work = [&](int q) {
+        std::vector<std::string_view> t;
+        std::vector<BoundRec>& out = parts[size_t(q)];
+        std::vector<std::string>& msg = errs[size_t(q)];
+        out.reserve((cut[size_t(q) + 1] - cut[size_t(q)]) / 12 + 16);
+        for (size_t pos = cut[size_t(q)]; pos < cut[size_t(q) + 1];) {
+            size_t nl = buf.find('\n', pos);
+            if (nl == std::string::npos || nl > cut[size_t(q) + 1]) nl = cut[size_t(q) + 1];
+            std::string_view line(buf.data() + pos, nl - pos);
+            pos = nl + 1;
+            if (!line.empty() && line.back() == '\r') line.remove_suffix(1);
+            if (line.find_first_not_of(" \t") == std::string_view::npos || line[0] == '*') continue;
+            split(line, "BOUNDS", false, t);
+            BoundRec r;
+            auto fail = [&](std::string m, bool early) {
+                r.err = int(msg.size()), r.early = early;
+                msg.push_back(std::move(m));
+            };
+            const std::string_view type = t.empty() ? std::string_view() : t[0];
+            const bool no_value = type == "FR" || type == "MI" || type == "PL" || type == "BV";
+            std::string_view col, val;
+            if (t.size() == 4) {
+                r.set = t[1], col = t[2], val = t[3];
+            } else if (t.size() == 3) {
+                if (no_value) r.set = t[1], col = t[2];
+                else col = t[1], val = t[2];
+            } else if (t.size() == 2) {
+                col = t[1];
+            } else {
+                fail("bad BOUNDS line", true);
+            }
+            if (r.err < 0) {
+                const int* jc = col_of(col);
+                if (!jc) {
+                    fail("unknown column '" + std::string(col) + "' in BOUNDS", false);
+                } else {
+                    r.col = *jc;
+                    try {
+                        r.v = no_value || val.empty() ? 0 : parse_number(val);
+                        for (int k = 0; k < 9; ++k)
+                            if (type == kBoundTypes[k]) r.type = k;
+                        if (r.type < 0) fail("unsupported bound type " + std::string(type), false);
+                    } catch (const ParseError& ex) {
+                        fail(ex.what(), false);
+                    }
+                }
+            }
+            out.push_back(r);
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int q = 1; q < threads; ++q) pool.emplace_back(work, q);
+    work(0);
+    for (auto& th : pool) th.join();
+}
+
 std::string read_file(const std::string& path) {
     std::ifstream in(path, std::ios::binary);
     if (!in) throw ParseError("cannot open " + path);
@@ -281,6 +377,20 @@ Model parse(const std::string& path, bool fixed) {
         if (free_rows.count(nm)) return -2;
         throw ParseError("unknown row '" + std::string(nm) + "'");
     };
+    auto apply_bound = [&](int j, std::string_view type, double v) {  // one BOUNDS entry, in file order
+        double &lo = md.col_lo[size_t(j)], &up = md.col_up[size_t(j)];
+        if (type == "BV" || type == "LI" || type == "UI") md.is_int[size_t(j)] = 1;
+        if (type == "LO" || type == "LI") lo = v;
+        else if (type == "UP" || type == "UI") {
+            up = v;
+            if (v < 0 && lo == 0) lo = -kInf;
+        } else if (type == "FX") lo = up = v;
+        else if (type == "FR") lo = -kInf, up = kInf;
+        else if (type == "MI") lo = -kInf;
+        else if (type == "PL") up = kInf;
+        else if (type == "BV") lo = 0, up = 1;
+        else throw ParseError("unsupported bound type " + std::string(type));
+    };
     auto col_of = [&](std::string_view nm) {
         const int* c = col_id.find(nm);
         if (!c) throw ParseError("unknown column '" + std::string(nm) + "'");
@@ -323,16 +433,7 @@ Model parse(const std::string& path, bool fixed) {
             if ((section == "ROWS" || section == "COLUMNS") && !seen.insert(section).second)
                 throw ParseError("section " + section + " appears twice");
             if (section == "COLUMNS" && !fixed) {  // the bulk of a file: tokenised in parallel, merged in order
-                size_t end = pos;
-                while (end < buf.size()) {
-                    size_t nl = buf.find('\n', end);
-                    if (nl == std::string::npos) nl = buf.size();
-                    std::string_view l(buf.data() + end, nl - end);
-                    if (!l.empty() && l.back() == '\r') l.remove_suffix(1);
-                    if (is_header(l)) break;
-                    end = nl + 1;
-                }
-                end = std::min(end, buf.size());
+                const size_t end = section_end(buf, pos);
                 std::vector<std::vector<ColRec>> parts;
                 const int nt = int(std::max<size_t>(1, std::min<size_t>(size_t(host_threads()), (end - pos) >> 20)));
                 if (nt > 1 && tokenize_columns(buf, pos, end, nt, row_of, parts)) {
@@ -360,6 +461,28 @@ Model parse(const std::string& path, bool fixed) {
                         if (c.row == -1) md.cost[j] += c.v;
                         else if (c.row >= 0) pending.push_back({c.row, c.v});
                     }
+                    pos = end;
+                }
+            }
+            if (section == "BOUNDS" && !fixed) {  // one line per bounded column: tokenised in parallel as well
+                const size_t end = section_end(buf, pos);
+                const int nt = int(std::max<size_t>(1, std::min<size_t>(size_t(host_threads()), (end - pos) >> 20)));
+                if (nt > 1) {
+                    std::vector<std::vector<BoundRec>> parts;
+                    std::vector<std::vector<std::string>> errs;
+                    tokenize_bounds(buf, pos, end, nt, [&](std::string_view nm) { return col_id.find(nm); }, parts,
+                                    errs);
+                    if (md.col_lo.empty()) {
+                        md.col_lo.assign(md.col_names.size(), 0);
+                        md.col_up.assign(md.col_names.size(), kInf);
+                    }
+                    for (size_t q = 0; q < parts.size(); ++q)
+                        for (const BoundRec& r : parts[q]) {
+                            if (r.err >= 0 && r.early) throw ParseError(errs[q][size_t(r.err)]);
+                            if (!r.set.empty() && !first_set(bound_set, r.set)) continue;
+                            if (r.err >= 0) throw ParseError(errs[q][size_t(r.err)]);
+                            apply_bound(r.col, kBoundTypes[r.type], r.v);
+                        }
                     pos = end;
                 }
             }
@@ -457,20 +580,7 @@ Model parse(const std::string& path, bool fixed) {
             if (!set.empty() && !first_set(bound_set, set)) continue;
             const int* jc = col_id.find(col);
             if (!jc) throw ParseError("unknown column '" + std::string(col) + "' in BOUNDS");
-            int j = *jc;
-            double v = no_value || val.empty() ? 0 : parse_number(val);
-            double &lo = md.col_lo[j], &up = md.col_up[j];
-            if (type == "BV" || type == "LI" || type == "UI") md.is_int[j] = 1;
-            if (type == "LO" || type == "LI") lo = v;
-            else if (type == "UP" || type == "UI") {
-                up = v;
-                if (v < 0 && lo == 0) lo = -kInf;
-            } else if (type == "FX") lo = up = v;
-            else if (type == "FR") lo = -kInf, up = kInf;
-            else if (type == "MI") lo = -kInf;
-            else if (type == "PL") up = kInf;
-            else if (type == "BV") lo = 0, up = 1;
-            else throw ParseError("unsupported bound type " + std::string(type));
+            apply_bound(*jc, type, no_value || val.empty() ? 0 : parse_number(val));
         } else if (section == "QUAD") {
             if (t.size() != 3) throw ParseError("bad quadratic objective line");
             int a = col_of(t[0]), b = col_of(t[1]);

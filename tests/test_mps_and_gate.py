@@ -270,3 +270,73 @@ def test_reader_parallel_columns_errors(engine_lib, tmp_path, edit, msg):
         pdhg.read_mps(write(tmp_path, "\n".join(lines)))
     free_msg = str(e.value).split(" (free format)")[0]
     assert e.value.code == pdhg.ERR_PARSE and msg in free_msg, str(e.value)
+
+
+def _big_bounds_text(n=120_000, extra=""):
+    """A model whose BOUNDS section is several MB (tokenised on several threads): every bound type, a second bound
+    set (ignored), columns bounded twice, UP < 0 on a zero lower bound. Returns (text, expected lo, up, is_int)."""
+    types = ["LO", "UP", "FX", "FR", "MI", "PL", "BV", "LI", "UI"]
+    inf = float("inf")
+    lo, up, isint = np.zeros(n), np.full(n, inf), np.zeros(n, np.uint8)
+    cols = "\n".join(f"    X{j}  R0  1" for j in range(n))
+    bl = []
+
+    def add(t, j, v=None, bset="BND"):
+        bl.append(f" {t} {bset} X{j}" + ("" if v is None else f" {v}"))
+        if bset != "BND":
+            return
+        if t in ("BV", "LI", "UI"):
+            isint[j] = 1
+        if t in ("LO", "LI"):
+            lo[j] = v
+        elif t in ("UP", "UI"):
+            up[j] = v
+            if v < 0 and lo[j] == 0:
+                lo[j] = -inf
+        elif t == "FX":
+            lo[j] = up[j] = v
+        elif t == "FR":
+            lo[j], up[j] = -inf, inf
+        elif t == "MI":
+            lo[j] = -inf
+        elif t == "PL":
+            up[j] = inf
+        elif t == "BV":
+            lo[j], up[j] = 0, 1
+    for j in range(n):
+        t = types[j % 9]
+        v = None if t in ("FR", "MI", "PL", "BV") else (-2.5 if j % 18 == 1 else float(j % 97) + 0.5)
+        add(t, j, v)
+        if j % 7 == 3:
+            add("UP", j, 99.0, bset="OTHER")  # a second bound set: ignored
+        if j % 11 == 5:
+            add("UP", j, float(j % 13) + 100.0)  # bounded twice: applied in file order
+    text = ("NAME BIGB\nROWS\n N OBJ\n L R0\nCOLUMNS\n" + cols + "\nRHS\n    RHS R0 1\nBOUNDS\n" + "\n".join(bl)
+            + "\n" + extra + "ENDATA\n")
+    return text, lo, up, isint
+
+
+def test_reader_parallel_bounds(engine_lib, tmp_path):
+    text, lo, up, isint = _big_bounds_text()
+    assert len(text.split("BOUNDS\n")[1]) > 2 << 20
+    m = pdhg.read_mps(write(tmp_path, text))
+    assert np.array_equal(m.col_lo, lo) and np.array_equal(m.col_up, up) and np.array_equal(m.is_int, isint)
+
+
+@pytest.mark.parametrize("extra,msg", [
+    (" UP BND NOSUCH 1\n", "unknown column 'NOSUCH' in BOUNDS"),
+    (" UP OTHER NOSUCH 1\n UP OTHER X1 1.2.3\n", None),  # lines of another bound set are skipped unchecked
+    (" UP\n", "bad BOUNDS line"),
+    (" XX BND X1 1\n", "unsupported bound type XX"),
+    (" UP BND X1 1.2.3\n", "bad number"),
+    (" UP BND NOSUCH 1.2.3\n UP\n", "unknown column 'NOSUCH'"),  # the first error in file order
+])
+def test_reader_parallel_bounds_errors(engine_lib, tmp_path, extra, msg):
+    text, lo, up, isint = _big_bounds_text(extra=extra)
+    if msg is None:
+        m = pdhg.read_mps(write(tmp_path, text))
+        assert np.array_equal(m.col_up, up)
+        return
+    with pytest.raises(pdhg.TaralError) as e:
+        pdhg.read_mps(write(tmp_path, text))
+    assert e.value.code == pdhg.ERR_PARSE and msg in str(e.value).split(" (free format)")[0], str(e.value)
