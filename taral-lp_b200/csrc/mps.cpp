@@ -111,6 +111,21 @@ class NameTable {
         }
     }
     bool count(std::string_view k) const { return find(k) != nullptr; }
+    // Adds k unless it is present (one probe sequence); returns -1 when added, else the index k already has.
+    int add_if_absent(std::string_view k) {
+        if (2 * (name_.size() + 1) > slot_.size()) rehash(2 * slot_.size());
+        const uint64_t h = hash(k);
+        const uint32_t tag = uint32_t(h >> 32);
+        size_t i = h & mask_;
+        for (;; i = (i + 1) & mask_) {
+            const Slot& s = slot_[i];
+            if (s.idx < 0) break;
+            if (s.tag == tag && name_[size_t(s.idx)] == k) return s.idx;
+        }
+        slot_[i] = {tag, int(name_.size())};
+        name_.push_back(k);
+        return -1;
+    }
     int add(std::string_view k) {  // k must not be present; indices are 0, 1, 2, ... in insertion order
         if (2 * (name_.size() + 1) > slot_.size()) rehash(2 * slot_.size());
         const int v = int(name_.size());
@@ -447,11 +462,10 @@ Model parse(const std::string& path, bool fixed) {
                         if (cur >= 0 && c.col == cur_name) {
                             j = cur;
                         } else {
-                            if (col_id.count(c.col))
+                            if (col_id.add_if_absent(c.col) >= 0)
                                 throw ParseError("column '" + std::string(c.col) + "' is listed in two separate blocks");
                             close_column();
                             j = int(md.col_names.size());
-                            col_id.add(c.col);
                             md.col_names.emplace_back(c.col);
                             cur_name = c.col;
                             md.cost.push_back(0);
@@ -521,11 +535,10 @@ Model parse(const std::string& path, bool fixed) {
             if (cur >= 0 && t[0] == cur_name) {
                 j = cur;
             } else {
-                if (col_id.count(t[0]))
+                if (col_id.add_if_absent(t[0]) >= 0)
                     throw ParseError("column '" + std::string(t[0]) + "' is listed in two separate blocks");
                 close_column();
                 j = int(md.col_names.size());
-                col_id.add(t[0]);
                 md.col_names.emplace_back(t[0]);
                 cur_name = t[0];
                 md.cost.push_back(0);
