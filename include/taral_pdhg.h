@@ -165,7 +165,9 @@ int taral_pdhg_solve_warm(const taral_model* md, const taral_options* o, const d
 
 /* Backend-level entries that take the solver's options and outcome types. */
 /* Input gate + scaling (gpu/pdhg.cu:80-133) + pdhg_create for a column-wise model: the device context of the
- * model's scaled problem. bnorm / cnorm (may be NULL) receive the original-space norms pdhg_solve_ctx needs. */
+ * model's scaled problem. bnorm / cnorm (may be NULL) receive the original-space norms pdhg_solve_ctx needs. An FP32
+ * context may hold the rows in another order internally (sorted by length); every vector passed in or out
+ * (pdhg_start, pdhg_download) is in the model's row order. */
 int pdhg_create_model(const taral_model* md, int precision, int eval_freq, unsigned flags, pdhg_ctx** out,
                       double* bnorm, double* cnorm);
 /* run<B> (gpu/pdhg.cu:761-849) on an existing context: power iteration, step sizes, the eval / terminate /
