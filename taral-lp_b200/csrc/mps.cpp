@@ -452,6 +452,16 @@ Model parse(const std::string& path, bool fixed) {
                 std::vector<std::vector<ColRec>> parts;
                 const int nt = int(std::max<size_t>(1, std::min<size_t>(size_t(host_threads()), (end - pos) >> 20)));
                 if (nt > 1 && tokenize_columns(buf, pos, end, nt, row_of, parts)) {
+                    size_t recs = 0, starts = 0;  // capacity: entries, and an upper bound on the new columns
+                    for (const std::vector<ColRec>& part : parts) {
+                        recs += part.size();
+                        std::string_view prev;
+                        for (const ColRec& c : part)
+                            if (!c.kind && c.col != prev) ++starts, prev = c.col;
+                    }
+                    md.row_idx.reserve(md.row_idx.size() + recs), md.val.reserve(md.val.size() + recs);
+                    md.col_names.reserve(md.col_names.size() + starts), md.cost.reserve(md.cost.size() + starts);
+                    md.is_int.reserve(md.is_int.size() + starts), md.col_ptr.reserve(md.col_ptr.size() + starts);
                     for (const std::vector<ColRec>& part : parts)
                     for (const ColRec& c : part) {
                         if (c.kind) {
