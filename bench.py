@@ -169,11 +169,29 @@ def cpu_solvers(cap_s=120.0):
     return out
 
 
+_MPS_FILES = []  # (model, path): each model the reference binary reads is written once per process
+_MPS_DIR = None
+
+
+def mps_file(lp):
+    """The model as an MPS file, written on first use into a temporary directory that lives as long as the process."""
+    global _MPS_DIR
+    for m, f in _MPS_FILES:
+        if m is lp:
+            return f
+    if _MPS_DIR is None:
+        _MPS_DIR = tempfile.TemporaryDirectory()
+    f = Path(_MPS_DIR.name) / f"m{len(_MPS_FILES)}.mps"
+    lp.write_mps(f)
+    _MPS_FILES.append((lp, f))
+    return f
+
+
 def run_reference_sample(lp, iters, threads):
     """The reference CPU PDHG (--device cpu, FP64) on the model for `iters` iterations; per-iteration seconds."""
+    f = mps_file(lp)
     with tempfile.TemporaryDirectory() as td:
-        f, j = Path(td) / "m.mps", Path(td) / "r.json"
-        lp.write_mps(f)
+        j = Path(td) / "r.json"
         subprocess.run([str(ref_binary()), str(f), "--device", "cpu", "--threads", str(threads), "--tol", "1e-6",
                         "--max-iter", str(iters), "--json", str(j)], check=True, stdout=subprocess.DEVNULL,
                        timeout=1800)
@@ -186,9 +204,9 @@ def run_reference_sample(lp, iters, threads):
 def run_reference_gpu(lp, limit_s=120.0):
     """The reference's own GPU backend (oracle/_ref/pdhg --device gpu, its default FP64, built for sm_100a from its
     sources) on the model to 1e-6, capped at limit_s: its JSON report, or {"status": "failed: ..."}."""
+    f = mps_file(lp)
     with tempfile.TemporaryDirectory() as td:
-        f, j = Path(td) / "m.mps", Path(td) / "r.json"
-        lp.write_mps(f)
+        j = Path(td) / "r.json"
         try:
             subprocess.run([str(ref_binary()), str(f), "--device", "gpu", "--tol", "1e-6", "--time-limit", str(limit_s),
                             "--json", str(j)], check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL,
