@@ -291,11 +291,11 @@ def traffic_from_profile():
 
 
 def gather_floor(nnz):
-    """The random-gather floor of this GPU, measured now by the committed probe (bin/gather_probe: `nnz` int32 index +
+    """The random-gather floor of this GPU, measured now by the committed probe (bin/gather_floor: `nnz` int32 index +
     float value pairs and one uniformly random float gather each, L2 flushed before every launch): {vector length:
     microseconds per launch} for the vector lengths 500,000 (x, gathered by the row phase) and 200,000 (z, column
     phase), or None when the probe is missing or fails."""
-    probe = ROOT / "taral-lp_b200" / "bin" / "gather_probe"
+    probe = ROOT / "taral-lp_b200" / "bin" / "gather_floor"
     if not probe.exists():
         return None
     try:
@@ -411,7 +411,7 @@ def our_arm(args, rank, world, dist):
                              "row_us": floor.get(n), "col_us": floor.get(m),
                              "row_frac": floor[n] / (row_ms * 1e3) if n in floor else None,
                              "col_frac": floor[m] / (col_ms * 1e3) if m in floor else None,
-                             "source": "bin/gather_probe in this run: the same count of random 4-byte gathers "
+                             "source": "bin/gather_floor in this run: the same count of random 4-byte gathers "
                                        "with their index/value stream, L2 flushed before each launch"}},
             "cpu_baseline": cpu if cpu is None or solvers is None else {**cpu, "solvers_small_lp": solvers},
             "gpu_launches": launches,

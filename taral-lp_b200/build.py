@@ -1,5 +1,6 @@
 """Build the engine in-tree: lib/libtaral_pdhg.so (CUDA kernels for sm_100a + host code + C ABI), bin/pdhg (the
-CLI) and bin/gather_probe (the random-gather floor measurement of the SpMV phases).
+CLI) and bin/gather_floor (probe/gather_floor.cu: the random-gather floor the benchmark measures beside the SpMV
+phases; a measurement tool, not part of the library).
 
 nvcc cross-compiles without a GPU. Objects are rebuilt only when a source or header is newer.
 Usage: python taral-lp_b200/build.py [--force]
@@ -18,7 +19,7 @@ CSRC = PKG / "csrc"
 OBJ = PKG / "_build"
 LIB = PKG / "lib" / "libtaral_pdhg.so"
 CLI = PKG / "bin" / "pdhg"
-PROBE = PKG / "bin" / "gather_probe"
+PROBE = PKG / "bin" / "gather_floor"
 NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-O3", "-I", str(ROOT / "include")]
@@ -58,7 +59,7 @@ def build(force: bool = False) -> Path:
     if force or _stale(CLI, [cli_o, LIB]):
         subprocess.run([NVCC, *ARCH, "-o", str(CLI), str(cli_o), "-L", str(LIB.parent), "-ltaral_pdhg",
                         "-Xlinker", "-rpath,$ORIGIN/../lib"], check=True)
-    probe_src = CSRC / "gather_probe.cu"
+    probe_src = PKG / "probe" / "gather_floor.cu"
     if force or _stale(PROBE, [probe_src]):
         subprocess.run([NVCC, *ARCH, "-O3", "-std=c++17", "-o", str(PROBE), str(probe_src)], check=True)
     return LIB

@@ -117,7 +117,6 @@ struct CudaError {
 struct DevMat {
     int rows = 0, maxrow = 0;  // maxrow: the longest row's nonzeros
     bool per_thread = false;   // SpMV by k_rowthread (one thread per row) instead of the row blocks
-    int split = 0;             // rows [0, split) by k_rowthread, the row blocks cover [split, rows)
     int64_t nnz = 0;
     int *ptr = nullptr, *idx = nullptr;
     int4* blk = nullptr;
@@ -208,13 +207,12 @@ struct Engine final : EngineBase {
     // and the column phase's gathers of z concentrate on a contiguous tail (a long row of A is gathered by many
     // columns), which L1 and L2 serve far better. Every row's entries keep their order and A^T's entries keep
     // theirs (renumbered), so both phases add the same products in the same order as in the model's row order;
-    // only the FP64 KKT sums over rows change order. TARAL_ROWORDER=0 keeps the model's order; 2 also runs the
-    // short prefix on the thread-per-row kernel (measured slower). rperm[k] = model row at position k.
+    // only the FP64 KKT sums over rows change order. TARAL_ROWORDER=0 keeps the model's order. rperm[k] = model row
+    // at position k.
     std::vector<int> rperm;
-    int rsplit = 0;
     bool order_rows(const Csr& a, const Csr& at, Csr& ap, Csr& atp) {
-        rperm.clear(), rsplit = 0;
-        const char* e = std::getenv("TARAL_ROWORDER");  // 0 off, 1 (default) sorted rows, 2 plus the thread prefix
+        rperm.clear();
+        const char* e = std::getenv("TARAL_ROWORDER");  // 0 off, otherwise (default) rows sorted by length
         const int mode = e ? std::atoi(e) : 1;
         if (sizeof(T) != sizeof(float) || mode <= 0 || a.rows == 0) return false;
         const int rows = a.rows;
@@ -239,7 +237,7 @@ struct Engine final : EngineBase {
         atp.rows = at.rows, atp.ptr = at.ptr, atp.val = at.val;
         atp.idx.resize(at.idx.size());
         for (size_t q = 0; q < at.idx.size(); ++q) atp.idx[q] = inv[size_t(at.idx[q])];
-        rperm = std::move(perm), rsplit = mode == 2 ? split : 0;
+        rperm = std::move(perm);
         return true;
     }
     std::vector<double> to_internal(const std::vector<double>& v) const {  // model row order -> internal
@@ -253,14 +251,13 @@ struct Engine final : EngineBase {
         return o;
     }
     // Row pointers, column indices and row blocks of one matrix on the device; the values are left to the caller.
-    DevMat upload_structure(const Csr& a, int split = 0) {
+    DevMat upload_structure(const Csr& a) {
         DevMat d;
-        d.rows = a.rows, d.nnz = int64_t(a.idx.size()), d.split = split;
+        d.rows = a.rows, d.nnz = int64_t(a.idx.size());
         std::vector<int> p32(size_t(a.rows) + 1);
         for (int r = 0; r <= a.rows; ++r) p32[r] = int(a.ptr[r]);
         for (int r = 0; r < a.rows; ++r) d.maxrow = std::max(d.maxrow, p32[r + 1] - p32[r]);
-        std::vector<int4> blk = build_row_blocks(a.ptr.data() + split, a.rows - split);
-        for (int4& b : blk) b.x += split;  // rows counted from the split
+        std::vector<int4> blk = build_row_blocks(a.ptr.data(), a.rows);
         d.nblk = int(blk.size());
         d.ptr = alloc<int>(p32.size()), d.idx = alloc<int>(size_t(d.nnz)), d.blk = alloc<int4>(blk.size());
         CK(cudaMemcpyAsync(d.ptr, p32.data(), p32.size() * sizeof(int), cudaMemcpyHostToDevice, st));
@@ -287,7 +284,7 @@ struct Engine final : EngineBase {
         const Csr& uAT = reorder ? hATp : hAT;
         double hs = since(t0);
         begin(md.m, md.n, freq, flags);
-        A = upload_structure(uA, reorder ? rsplit : 0), AT = upload_structure(uAT);
+        A = upload_structure(uA), AT = upload_structure(uAT);
         const int64_t nz = int64_t(hA.val.size());
         P.m = m, P.n = n;
         P.Dr.resize(size_t(m)), P.Dc.resize(size_t(n));
@@ -476,11 +473,6 @@ struct Engine final : EngineBase {
     // ------------------------------------------------------------------ SpMV-shaped launches
     template <class X, class E>
     void rowblock(const DevMat& a, const X* xin, const E& epi, const int* skip = nullptr) {
-        if (a.split > 0) {  // the short-row prefix of a length-ordered matrix
-            k_rowthread<T, X, E><<<(a.split + kThreads - 1) / kThreads, kThreads, 0, st>>>(
-                a.split, a.ptr, a.idx, static_cast<const T*>(a.val), xin, skip, epi);
-            ++launches;
-        }
         if (a.nblk == 0) return;
         if (a.per_thread)
             k_rowthread<T, X, E><<<(a.rows + kThreads - 1) / kThreads, kThreads, 0, st>>>(

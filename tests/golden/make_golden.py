@@ -1,7 +1,7 @@
 #!/usr/bin/env python3
 """Regenerate the golden fixtures of tests/golden/ from the reference implementation.
 
-Needs the reference checkout (REF, default /root/reference) and the reference binaries built from it by
+Needs the reference checkout (REF, default: the directory "reference" beside this repository's checkout) and the reference binaries built from it by
 ``make -C oracle ref`` (oracle/_ref/pdhg, oracle/_ref/taral). Writes:
 
 * gen_lp_sha256.json     sha256 of the MPS text that the reference's gpu/gen_lp.py writes for a few seeds
@@ -32,7 +32,7 @@ from pathlib import Path
 import numpy as np
 
 ROOT = Path(__file__).resolve().parents[2]
-REF = Path(os.environ.get("REF", "/root/reference"))
+REF = Path(os.environ.get("REF", str(Path(__file__).resolve().parents[3] / "reference")))
 OUT = Path(__file__).resolve().parent
 PDHG = ROOT / "oracle" / "_ref" / "pdhg"
 TARAL = ROOT / "oracle" / "_ref" / "taral"

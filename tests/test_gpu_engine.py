@@ -176,8 +176,8 @@ def test_row_thread_kernel_is_bit_identical(engine_lib, monkeypatch, precision):
 
 
 def test_row_order_fp32(engine_lib, monkeypatch):
-    # FP32 contexts may run with their rows sorted by length (TARAL_ROWORDER=1: a thread-per-row prefix, staged
-    # blocks over the long tail): the same answer, and the dual vector comes back in the model's row order
+    # FP32 contexts run with their rows sorted by length inside the engine (TARAL_ROWORDER=1, the default; the same
+    # kernels as in the model's order): the same answer, and the dual vector comes back in the model's row order
     lp = lpgen.planted(20_000, 50_000, 10, seed=4, zipf=1.2, cap=2000, floor=5)
     monkeypatch.setenv("TARAL_ROWORDER", "0")
     r0, x0, y0 = pdhg.solve(lp, tol=1e-6, precision=pdhg.FP32, time_limit=120)
