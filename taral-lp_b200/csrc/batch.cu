@@ -43,15 +43,15 @@ struct BatchError {
         if (e_ != cudaSuccess) throw BatchError{std::string(#call) + ": " + cudaGetErrorString(e_)};        \
     } while (0)
 
-// Per-instance driver state (device resident, FP64 where the reference uses double).
+// Per-instance driver state (device resident, FP64): the restart schedule shared with the single-LP driver
+// (schedule.hpp: weight, step scale, anchor, iteration counters) and what the batch keeps beside it -- the averages'
+// scale f = 1 / (iterations since the restart), f at the last restart, the stopping test's norms, the better
+// point's residuals, the operator norm and the status flags.
 struct InstState {
-    double w, eta, k_last, k_prev, f, f_restart, bnorm, cnorm, best_p, best_d, best_g, norm;
-    long long it, n_since;
-    int status, restarts, avg_final, running, restart_flag, pad;
+    Schedule sch;
+    double f, f_restart, bnorm, cnorm, best_p, best_d, best_g, norm;
+    int status, avg_final, running, restart_flag;
 };
-
-__device__ __forceinline__ double dmax(double a, double b) { return a < b ? b : a; }  // std::max semantics
-__device__ __forceinline__ double dmin(double a, double b) { return b < a ? b : a; }  // std::min semantics
 
 // ---------------------------------------------------------------------------------------------- batch kernels
 // ---------------------------------------------------------------------------------------------- pack layout
@@ -263,71 +263,39 @@ __global__ void k_eval_finish(int ninst, const int2* __restrict__ where, const i
     kkt[inst * 10 + lane] = s;
 }
 
-__device__ __forceinline__ double wkkt(const double* k, double w) {
-    double g = k[POBJ] - (k[DROW] + k[DCOL]);
-    return sqrt(w * k[PR2S] + k[DR2S] / w + g * g);
-}
-
-// The per-block decision of gpu/pdhg.cu:806-842 for every running instance (one thread each).
+// The schedule's decision after a block (schedule.hpp, judge_block) for every running instance, one thread each.
+// The deadline is compared with %globaltimer (0: none). rflag[i]: where instance i restarts (RestartTo).
 template <class T>
 __global__ void k_decide(int ninst, InstState* st, const double* __restrict__ kc_all, const double* __restrict__ ka_all,
                          double* par, int* running, int* rflag, double tol, double row_rel, long long max_iter,
                          const unsigned long long* deadline) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= ninst) return;
-    rflag[i] = 0;
+    rflag[i] = kNoRestart;
     InstState& s = st[i];
     if (!s.running) return;
-    const double* kc = kc_all + 10 * i;
-    const double* ka = ka_all + 10 * i;
-    auto rel = [&](const double* k, double& p, double& d, double& g) {
-        double po = k[POBJ], du = k[DROW] + k[DCOL];
-        double prow = row_rel > 0 ? sqrt(k[PR2R]) / row_rel : 0;
-        p = dmax(sqrt(k[PR2O]) / (1 + s.bnorm), prow), d = sqrt(k[DR2O]) / (1 + s.cnorm);
-        g = fabs(po - du) / (1 + fabs(po) + fabs(du));
-    };
-    double cp, cd, cg, ap, ad, ag;
-    rel(kc, cp, cd, cg), rel(ka, ap, ad, ag);
-    double wc_ = dmax(cp, dmax(cd, cg)), wa_ = dmax(ap, dmax(ad, ag));
-    bool use_avg = wa_ < wc_;
-    s.best_p = use_avg ? ap : cp, s.best_d = use_avg ? ad : cd, s.best_g = use_avg ? ag : cg;
-    s.avg_final = use_avg;
-    double best = use_avg ? wa_ : wc_;
     unsigned long long now;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
-    if (!isfinite(wc_) && !isfinite(wa_)) s.status = TARAL_NUMERICAL_FAILURE, s.running = 0;
-    else if (best <= tol) s.status = TARAL_NEAR_OPTIMAL, s.running = 0;
-    else if (*deadline && now > *deadline) s.status = TARAL_TIME_LIMIT, s.running = 0;
-    else if (s.it >= max_iter) s.status = TARAL_ITERATION_LIMIT, s.running = 0;
-    if (!s.running) {
-        running[i] = 0;
+    const StopRule rule{tol, row_rel, s.bnorm, s.cnorm, max_iter};
+    const BlockDecision d = judge_block(s.sch, kc_all + 10 * i, ka_all + 10 * i, rule, *deadline && now > *deadline);
+    s.best_p = d.best.primal, s.best_d = d.best.dual, s.best_g = d.best.gap, s.avg_final = d.average_better;
+    if (d.status >= 0) {
+        s.status = d.status, s.running = 0, running[i] = 0;
         return;
     }
-    double w = s.w, wc = wkkt(kc, w), wa = wkkt(ka, w);
-    bool cand_avg = wa < wc;
-    const double* kk = cand_avg ? ka : kc;
-    double kcand = dmin(wa, wc);
-    bool restart = double(s.n_since) >= 0.36 * double(s.it) || kcand <= 0.2 * s.k_last ||
-                   (kcand <= 0.8 * s.k_last && kcand > s.k_prev);
-    s.k_prev = kcand;
-    if (restart) {
-        double dx = sqrt(kk[DX2]), dz = sqrt(kk[DZ2]);
-        rflag[i] = cand_avg ? 2 : 1;
+    if (d.restart != kNoRestart) {
+        rflag[i] = d.restart;
         s.f_restart = s.f;
-        if (dx > 1e-10 && dz > 1e-10) {
-            w = exp(0.5 * log(dz / dx) + 0.5 * log(w));
-            s.w = w;
-            par[2 * i] = s.eta / w, par[2 * i + 1] = s.eta * w;
-        }
-        s.k_last = wkkt(kk, w), s.k_prev = INFINITY, s.n_since = 0, s.restarts++;
+        if (d.new_weight) par[2 * i] = s.sch.eta / s.sch.weight, par[2 * i + 1] = s.sch.eta * s.sch.weight;
     }
 }
 
 __global__ void k_advance(int ninst, InstState* st, int steps) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= ninst || !st[i].running) return;
-    st[i].it += steps, st[i].n_since += steps;
-    st[i].f = 1.0 / double(st[i].n_since);
+    Schedule& q = st[i].sch;
+    q.iterations += steps, q.since_restart += steps;
+    st[i].f = 1.0 / double(q.since_restart);
 }
 
 // Gather the per-instance f (running sums scale) into a flat array for the evaluation kernels.
@@ -438,7 +406,7 @@ __global__ void k_pack_out(const int4* __restrict__ blk, const int4* __restrict_
     PACK_ENTRIES(true)
     if (!live) return;
     const InstState& s = st[inst];
-    const double f = 1.0 / double(s.n_since > 1 ? s.n_since : 1);
+    const double f = 1.0 / double(s.sch.since_restart > 1 ? s.sch.since_restart : 1);
     for (int q = threadIdx.x; q < (nrows << lw); q += blockDim.x) {
         const int j = vbase + q;
         out[j] = s.avg_final ? xs[j] * f : double(x[j]);
@@ -449,7 +417,7 @@ __global__ void k_pack_out(const int4* __restrict__ blk, const int4* __restrict_
 __global__ void k_kkt_init(int ninst, InstState* st, const double* __restrict__ kc) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= ninst) return;
-    st[i].k_last = wkkt(kc + 10 * i, st[i].w), st[i].k_prev = INFINITY;
+    st[i].sch.anchor = weighted_error(kc + 10 * i, st[i].sch.weight), st[i].sch.previous = INFINITY;
 }
 
 __global__ void k_set_deadline(unsigned long long* d, unsigned long long left_ns) {
@@ -1104,26 +1072,15 @@ struct Batch final : BatchBase {
         std::vector<double> hpar(2 * size_t(ninst));
         for (int i = 0; i < ninst; ++i) {
             const Scaled& v = vecs[i];
-            double cs = 0, bs = 0;
-            for (double cv : v.c) cs += cv * cv;
-            for (int r = 0; r < v.m; ++r) {
-                double lo = v.rl[r], up = v.ru[r];
-                double q = std::isfinite(lo) && std::isfinite(up) ? std::max(std::fabs(lo), std::fabs(up))
-                           : std::isfinite(lo)                    ? std::fabs(lo)
-                           : std::isfinite(up)                    ? std::fabs(up)
-                                                                  : 0;
-                bs += q * q;
-            }
-            cs = std::sqrt(cs), bs = std::sqrt(bs);
+            StepScale sc = initial_steps(norms[i], v.c.data(), v.n, v.rl.data(), v.ru.data(), v.m);
+            if (w0 && std::isfinite(w0[i]) && w0[i] > 0) sc.weight = w0[i];  // caller's initial primal weight
             InstState& q = hs[i];
             std::memset(&q, 0, sizeof q);
+            q.sch.weight = sc.weight, q.sch.eta = sc.eta;  // anchor and previous: k_kkt_init, on the start point
             q.norm = norms[i];
-            q.eta = norms[i] > 0 ? 0.95 / norms[i] : 1.0;
-            q.w = cs > 1e-10 && bs > 1e-10 ? cs / bs : 1.0;
-            if (w0 && std::isfinite(w0[i]) && w0[i] > 0) q.w = w0[i];  // caller's initial primal weight
             q.bnorm = v.bnorm, q.cnorm = v.cnorm, q.running = 1, q.status = TARAL_ITERATION_LIMIT;
             q.best_p = q.best_d = q.best_g = kInf;
-            hpar[2 * i] = q.eta / q.w, hpar[2 * i + 1] = q.eta * q.w;
+            hpar[2 * i] = sc.eta / sc.weight, hpar[2 * i + 1] = sc.eta * sc.weight;
         }
         BK(cudaMemcpyAsync(st, hs.data(), ninst * sizeof(InstState), cudaMemcpyHostToDevice, s));
         BK(cudaMemcpyAsync(par, hpar.data(), hpar.size() * sizeof(double), cudaMemcpyHostToDevice, s));
@@ -1221,8 +1178,10 @@ struct Batch final : BatchBase {
             const InstState& q = fin[i];
             const Shared& sh = *mats[mat_of[i]];
             Outcome r;
-            r.status = q.status, r.iterations = q.it, r.restarts = q.restarts, r.from_average = q.avg_final != 0;
-            r.rel_primal = q.best_p, r.rel_dual = q.best_d, r.rel_gap = q.best_g, r.norm_a = q.norm, r.omega = q.w;
+            r.status = q.status, r.iterations = q.sch.iterations, r.restarts = q.sch.restarts;
+            r.from_average = q.avg_final != 0;
+            r.rel_primal = q.best_p, r.rel_dual = q.best_d, r.rel_gap = q.best_g, r.norm_a = q.norm;
+            r.omega = q.sch.weight;
             r.x.resize(size_t(models[i]->n)), r.z.resize(size_t(models[i]->m));
             for (int j = 0; j < models[i]->n; ++j) r.x[j] = hx[xidx(i, j)];
             for (int q = 0; q < models[i]->m; ++q) r.z[q] = hz[zidx(i, q)];

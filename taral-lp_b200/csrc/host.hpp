@@ -1,5 +1,6 @@
 // Host side of the PDHG path: problem format, scaling, options/outcome and the driver loop.
 #pragma once
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdint>
@@ -10,6 +11,7 @@
 #include <vector>
 
 #include "../../include/taral_pdhg.h"
+#include "schedule.hpp"
 
 namespace taral {
 
@@ -93,105 +95,54 @@ struct DriverData {
     static DriverData of(const Scaled& P) { return {P.m, P.n, P.c.data(), P.rl.data(), P.ru.data(), P.bnorm, P.cnorm}; }
 };
 
-// KKT scalar slots (gpu/pdhg.cu:136, 145).
-enum { PR2S, PR2O, PR2R, DROW, DZ2, DR2S, DR2O, POBJ, DCOL, DX2 };
-
-// The restarted-average PDHG driver (gpu/pdhg.cu:761-849), generic over a backend with the concept's methods
-// (power_norm, set_steps, start, iterate, eval_pair, restart, download). x0/z0: optional warm start (scaled
-// space). The stopping rule, restart rule and primal-weight update follow the reference line by line; the
-// KKT scalars of the current point and of the average come back together (one synchronisation per block).
+// The restarted-average PDHG on one LP (gpu/pdhg.cu:761-849 semantics), generic over a backend with the concept's
+// methods (power_norm, set_steps, start, iterate, eval, eval_pair, restart, download). x0 / z0: optional warm start
+// (scaled space). Blocks of eval_freq iterations alternate with one evaluation of the current point and of the
+// average (a single synchronisation) and the schedule's decision (schedule.hpp), which the backend then carries
+// out: a restart to the chosen point and, after a weight change, new step sizes.
 template <class B>
 Outcome run(B& b, const DriverData& P, const Options& o, double time_budget, const double* x0 = nullptr,
             const double* z0 = nullptr) {
-    Outcome r;
-    auto t0 = Clock::now();
-    r.norm_a = b.power_norm(200);
-    r.power_s = since(t0);
-    double eta = r.norm_a > 0 ? 0.95 / r.norm_a : 1.0;
-    double cs = 0, bs = 0;
-    for (int j = 0; j < P.n; ++j) cs += P.c[j] * P.c[j];
-    for (int i = 0; i < P.m; ++i) {
-        double lo = P.rl[i], up = P.ru[i];
-        double v = std::isfinite(lo) && std::isfinite(up) ? std::max(std::fabs(lo), std::fabs(up))
-                   : std::isfinite(lo)                    ? std::fabs(lo)
-                   : std::isfinite(up)                    ? std::fabs(up)
-                                                          : 0;
-        bs += v * v;
-    }
-    cs = std::sqrt(cs), bs = std::sqrt(bs);
-    double w = cs > 1e-10 && bs > 1e-10 ? cs / bs : 1.0;
-    b.set_steps(eta / w, eta * w);
+    Outcome out;
+    const auto t0 = Clock::now();
+    out.norm_a = b.power_norm(200);
+    out.power_s = since(t0);
+    const StepScale scale = initial_steps(out.norm_a, P.c, P.n, P.rl, P.ru, P.m);
+    b.set_steps(scale.eta / scale.weight, scale.eta * scale.weight);
     b.start(x0, z0);
-
-    auto wkkt = [&](const double* k) {
-        double g = k[POBJ] - (k[DROW] + k[DCOL]);
-        return std::sqrt(w * k[PR2S] + k[DR2S] / w + g * g);
-    };
-    struct Rel {
-        double p, d, g;
-        double worst() const { return std::max(p, std::max(d, g)); }
-    };
-    auto rel = [&](const double* k) {
-        double po = k[POBJ], du = k[DROW] + k[DCOL];
-        double prow = o.row_rel > 0 ? std::sqrt(k[PR2R]) / o.row_rel : 0;
-        return Rel{std::max(std::sqrt(k[PR2O]) / (1 + P.bnorm), prow), std::sqrt(k[DR2O]) / (1 + P.cnorm),
-                   std::fabs(po - du) / (1 + std::fabs(po) + std::fabs(du))};
-    };
-    double kc[10], ka[10];
-    b.eval(false, 1.0, kc);
-    double k_last = wkkt(kc), k_prev = kInf;
-    int64_t it = 0, n_since = 0;
-    bool avg_final = false;
-    Rel best{kInf, kInf, kInf};
-    for (;;) {
-        int steps = int(std::min<int64_t>(o.eval_freq, o.max_iter - it));
-        if (steps <= 0) break;
-        b.iterate(steps);
-        it += steps, n_since += steps;
-        double f = 1.0 / double(n_since);
-        b.eval_pair(f, kc, ka);
-        Rel rc = rel(kc), ra = rel(ka);
-        bool use_avg = ra.worst() < rc.worst();
-        best = use_avg ? ra : rc, avg_final = use_avg;
-        if (o.verbose && (it / o.eval_freq) % 50 == 0)
-            std::fprintf(stderr, "it %lld  w %.3e  cur %.2e %.2e %.2e  avg %.2e %.2e %.2e  pobj %.10g\n",
-                         (long long)it, w, rc.p, rc.d, rc.g, ra.p, ra.d, ra.g, kc[POBJ]);
-        if (!std::isfinite(rc.worst()) && !std::isfinite(ra.worst())) {
-            r.status = TARAL_NUMERICAL_FAILURE;
+    double cur[10], avg[10];
+    b.eval(false, 1.0, cur);
+    Schedule sch = make_schedule(scale, cur);
+    const StopRule rule{o.tol, o.row_rel, P.bnorm, P.cnorm, int64_t(o.max_iter)};
+    BlockDecision last{};
+    last.best = {kInf, kInf, kInf}, last.average_better = false;
+    while (sch.iterations < o.max_iter) {
+        const int block = int(std::min<int64_t>(o.eval_freq, o.max_iter - sch.iterations));
+        b.iterate(block);
+        sch.iterations += block, sch.since_restart += block;
+        const double f = 1.0 / double(sch.since_restart);
+        b.eval_pair(f, cur, avg);
+        last = judge_block(sch, cur, avg, rule, since(t0) > time_budget);
+        if (o.verbose && (sch.iterations / o.eval_freq) % 50 == 0)
+            std::fprintf(stderr, "[pdhg] iter=%lld weight=%.3e best(p,d,gap)=(%.2e, %.2e, %.2e) from=%s c'x=%.10g\n",
+                         (long long)sch.iterations, sch.weight, last.best.primal, last.best.dual, last.best.gap,
+                         last.average_better ? "average" : "current", cur[POBJ]);
+        if (last.status >= 0) {
+            out.status = last.status;
             break;
         }
-        if (best.worst() <= o.tol) {
-            r.status = TARAL_NEAR_OPTIMAL;
-            break;
-        }
-        if (since(t0) > time_budget) {
-            r.status = TARAL_TIME_LIMIT;
-            break;
-        }
-        if (it >= o.max_iter) break;
-        double wc = wkkt(kc), wa = wkkt(ka);
-        bool cand_avg = wa < wc;
-        const double* kk = cand_avg ? ka : kc;
-        double kcand = std::min(wa, wc);
-        bool restart = double(n_since) >= 0.36 * double(it) || kcand <= 0.2 * k_last ||
-                       (kcand <= 0.8 * k_last && kcand > k_prev);
-        k_prev = kcand;
-        if (restart) {
-            double dx = std::sqrt(kk[DX2]), dz = std::sqrt(kk[DZ2]);
-            b.restart(cand_avg, f);
-            if (dx > 1e-10 && dz > 1e-10) {
-                w = std::exp(0.5 * std::log(dz / dx) + 0.5 * std::log(w));
-                b.set_steps(eta / w, eta * w);
-            }
-            k_last = wkkt(kk), k_prev = kInf, n_since = 0, r.restarts++;
+        if (last.restart != kNoRestart) {
+            b.restart(last.restart == kRestartAverage, f);
+            if (last.new_weight) b.set_steps(sch.eta / sch.weight, sch.eta * sch.weight);
         }
     }
-    r.iterations = it;
-    r.rel_primal = best.p, r.rel_dual = best.d, r.rel_gap = best.g, r.omega = w, r.from_average = avg_final;
-    r.x.resize(P.n), r.z.resize(P.m);
-    b.download(avg_final, 1.0 / double(std::max<int64_t>(n_since, 1)), r.x.data(), r.z.data());
-    r.iterate_s = since(t0) - r.power_s;
-    return r;
+    out.iterations = sch.iterations, out.restarts = sch.restarts, out.omega = sch.weight;
+    out.rel_primal = last.best.primal, out.rel_dual = last.best.dual, out.rel_gap = last.best.gap;
+    out.from_average = last.average_better;
+    out.x.resize(size_t(P.n)), out.z.resize(size_t(P.m));
+    b.download(out.from_average, 1.0 / double(std::max<int64_t>(sch.since_restart, 1)), out.x.data(), out.z.data());
+    out.iterate_s = since(t0) - out.power_s;
+    return out;
 }
 
 // Original-space figures of finish() (gpu/pdhg.cu:866-876): x = Dc x_s, objective (long double), max row and

@@ -1,6 +1,6 @@
 // Host preprocessing: the CSR transposes of the model (gpu/pdhg.cu:55-70 semantics), the scaled vectors and norms
-// (gpu/pdhg.cu:113-133) given the scaling factors computed on the device (scaling.cuh), and the original-space check
-// of an answer (gpu/pdhg.cu:866-876).
+// (gpu/pdhg.cu:113-133 semantics) given the scaling factors computed on the device (scaling.cuh), and the
+// original-space check of an answer (gpu/pdhg.cu:866-876 semantics).
 #include <algorithm>
 #include <cmath>
 #include <thread>
@@ -85,71 +85,105 @@ void model_matrices(const taral_model& md, Csr& A, Csr& AT, int threads) {
     }
 }
 
-void scale_vectors(const taral_model& md, double sign, const std::vector<double>& Dr, const std::vector<double>& Dc,
-                   Scaled& P) {
-    P.m = md.m, P.n = md.n;
-    P.c.resize(size_t(P.n)), P.l.resize(size_t(P.n)), P.u.resize(size_t(P.n));
-    P.rl.resize(size_t(P.m)), P.ru.resize(size_t(P.m));
-    P.cnorm = P.bnorm = 0;
-    for (int j = 0; j < P.n; ++j) {
-        double c = sign * md.cost[j];
-        P.cnorm += c * c;
-        P.c[j] = c * Dc[j], P.l[j] = md.col_lo[j] / Dc[j], P.u[j] = md.col_up[j] / Dc[j];
+namespace {
+
+// sqrt of the sum of v(i)^2 over i = 0 .. count-1, accumulated in index order
+template <class V>
+double root_sum_squares(int count, V v) {
+    double acc = 0;
+    for (int i = 0; i < count; ++i) {
+        const double e = v(i);
+        acc += e * e;
     }
-    for (int i = 0; i < P.m; ++i) {
-        double lo = md.row_lo[i], up = md.row_up[i], b = 0;
-        if (std::isfinite(lo) && std::isfinite(up)) b = std::max(std::fabs(lo), std::fabs(up));
-        else if (std::isfinite(lo)) b = std::fabs(lo);
-        else if (std::isfinite(up)) b = std::fabs(up);
-        P.bnorm += b * b;
-        P.rl[i] = lo * Dr[i], P.ru[i] = up * Dr[i];
-    }
-    P.bnorm = std::sqrt(P.bnorm), P.cnorm = std::sqrt(P.cnorm);
+    return std::sqrt(acc);
 }
 
+// how far v lies outside [lo, hi] (negative inside), and the running maximum of such excesses from 0
+inline double excess(double lo, double v, double hi) { return std::max(lo - v, v - hi); }
+inline void keep_worst(double& worst, double e) { worst = std::max(worst, e); }
+
+// largest row excess of the activities a = A x, rows [i0, i1) of the unscaled row-wise copy A (each row's entries
+// in ascending column order, summed in that order)
+double row_excess_range(const taral_model& md, const Csr& A, const std::vector<double>& x, int i0, int i1) {
+    double worst = 0;
+    for (int i = i0; i < i1; ++i) {
+        double a = 0.0;
+        for (int64_t k = A.ptr[i]; k < A.ptr[i + 1]; ++k) a += A.val[k] * x[A.idx[k]];
+        keep_worst(worst, excess(md.row_lo[i], a, md.row_up[i]));
+    }
+    return worst;
+}
+
+}  // namespace
+
+// The scaled problem's vectors: c_s = sign c Dc, l_s = l / Dc, u_s = u / Dc, rl_s = rl Dr, ru_s = ru Dr, and the
+// stopping test's original-space norms ||sign c|| and ||b|| (b_i: the larger finite row bound in magnitude).
+void scale_vectors(const taral_model& md, double sign, const std::vector<double>& Dr, const std::vector<double>& Dc,
+                   Scaled& P) {
+    const int n = md.n, m = md.m;
+    P.m = m, P.n = n;
+    P.cnorm = root_sum_squares(n, [&](int j) { return sign * md.cost[j]; });
+    P.bnorm = root_sum_squares(m, [&](int i) { return bound_size(md.row_lo[i], md.row_up[i]); });
+    P.c.resize(size_t(n)), P.l.resize(size_t(n)), P.u.resize(size_t(n));
+    for (int j = 0; j < n; ++j) {
+        const double d = Dc[size_t(j)];
+        P.c[size_t(j)] = (sign * md.cost[j]) * d;
+        P.l[size_t(j)] = md.col_lo[j] / d;
+        P.u[size_t(j)] = md.col_up[j] / d;
+    }
+    P.rl.resize(size_t(m)), P.ru.resize(size_t(m));
+    for (int i = 0; i < m; ++i) {
+        const double d = Dr[size_t(i)];
+        P.rl[size_t(i)] = md.row_lo[i] * d;
+        P.ru[size_t(i)] = md.row_up[i] * d;
+    }
+}
+
+// The answer in original units and how well it satisfies the original model: x = Dc x_s, y = Dr z_s, the
+// objective c'x + obj_const accumulated in long double, the largest bound excess max(l - x, x - u) and the
+// largest row excess max(lo - a, a - up) of the activities a = A x, all from 0. The activities come from the
+// unscaled row-wise copy on several host threads when the set-up kept it (their sums add the same products in the
+// same order as a sweep over the model's columns), otherwise from one sweep over the columns.
 Finished finish_point(const taral_model& md, const Scaled& P, const Outcome& r) {
-    Finished f;
-    f.x.resize(size_t(P.n));
-    f.y.resize(size_t(P.m));
-    for (int j = 0; j < P.n; ++j) f.x[j] = r.x[j] * P.Dc[j];
-    for (int i = 0; i < P.m; ++i) f.y[i] = P.Dr[i] * r.z[i];
-    long double obj = md.obj_const;
-    for (int j = 0; j < P.n; ++j) obj += (long double)md.cost[j] * f.x[j];
-    double bviol = 0, rviol = 0;
-    bool finite = true;
-    for (int j = 0; j < P.n; ++j) {
-        bviol = std::max(bviol, std::max(md.col_lo[j] - f.x[j], f.x[j] - md.col_up[j]));
-        finite = finite && std::isfinite(f.x[j]);
+    const int n = P.n, m = P.m;
+    Finished out;
+    out.x.resize(size_t(n)), out.y.resize(size_t(m));
+    for (int j = 0; j < n; ++j) out.x[size_t(j)] = r.x[size_t(j)] * P.Dc[size_t(j)];
+    for (int i = 0; i < m; ++i) out.y[size_t(i)] = P.Dr[size_t(i)] * r.z[size_t(i)];
+
+    long double objective = md.obj_const;
+    for (int j = 0; j < n; ++j) objective += (long double)md.cost[j] * out.x[size_t(j)];
+    out.objective = double(objective);
+
+    bool all_finite = true;
+    for (int j = 0; j < n; ++j) {
+        const double v = out.x[size_t(j)];
+        keep_worst(out.max_bound_violation, excess(md.col_lo[j], v, md.col_up[j]));
+        all_finite = all_finite && std::isfinite(v);
     }
-    if (finite && P.a_original && P.m > 0) {
-        // Row activities from the unscaled row-wise copy: each row lists its entries in ascending column order, so
-        // its sequential sum adds the same products in the same order as the column sweep below (explicit zeros
-        // add nothing for finite x). Rows are split over threads; the maximum does not depend on the split.
-        const int nt = std::max(1, std::min(host_threads(), P.m / 4096));
-        std::vector<double> part(size_t(nt), 0.0);
-        auto work = [&](int q) {
-            const int i0 = int(int64_t(P.m) * q / nt), i1 = int(int64_t(P.m) * (q + 1) / nt);
-            double v = 0;
-            for (int i = i0; i < i1; ++i) {
-                double a = 0.0;
-                for (int64_t k = P.A.ptr[i]; k < P.A.ptr[i + 1]; ++k) a += P.A.val[k] * f.x[P.A.idx[k]];
-                v = std::max(v, std::max(md.row_lo[i] - a, a - md.row_up[i]));
-            }
-            part[q] = v;
+
+    if (all_finite && P.a_original && m > 0) {
+        // explicit zeros of the model add nothing to a sum of finite products; the maximum is split-independent
+        const int parts = std::max(1, std::min(host_threads(), m / 4096));
+        std::vector<double> worst(size_t(parts), 0.0);
+        auto part = [&](int q) {
+            worst[size_t(q)] = row_excess_range(md, P.A, out.x, int(int64_t(m) * q / parts),
+                                                int(int64_t(m) * (q + 1) / parts));
         };
-        std::vector<std::thread> pool;
-        for (int q = 1; q < nt; ++q) pool.emplace_back(work, q);
-        work(0);
-        for (auto& th : pool) th.join();
-        for (double v : part) rviol = std::max(rviol, v);
+        std::vector<std::thread> helpers;
+        for (int q = 1; q < parts; ++q) helpers.emplace_back(part, q);
+        part(0);
+        for (std::thread& h : helpers) h.join();
+        for (double w : worst) keep_worst(out.max_row_violation, w);
     } else {
-        std::vector<double> ax(size_t(P.m), 0.0);
-        for (int j = 0; j < P.n; ++j)
-            for (int64_t k = md.col_ptr[j]; k < md.col_ptr[j + 1]; ++k) ax[md.row_idx[k]] += md.val[k] * f.x[j];
-        for (int i = 0; i < P.m; ++i) rviol = std::max(rviol, std::max(md.row_lo[i] - ax[i], ax[i] - md.row_up[i]));
+        std::vector<double> activity(size_t(m), 0.0);
+        for (int j = 0; j < n; ++j) {
+            const double v = out.x[size_t(j)];
+            for (int64_t k = md.col_ptr[j]; k < md.col_ptr[j + 1]; ++k) activity[size_t(md.row_idx[k])] += md.val[k] * v;
+        }
+        for (int i = 0; i < m; ++i) keep_worst(out.max_row_violation, excess(md.row_lo[i], activity[size_t(i)], md.row_up[i]));
     }
-    f.objective = double(obj), f.max_row_violation = rviol, f.max_bound_violation = bviol;
-    return f;
+    return out;
 }
 
 const char* status_name(int s) {
