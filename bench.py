@@ -8,22 +8,31 @@ tolerance 1e-6, seeded synthetic data (seed = rank). One step = one full solve o
 * value -- the device-resident solve (power iteration, the PDHG loop with its restarts and evaluations, the
   final download of x and z) on a context created before the timed region; CUDA-event time on the engine's
   stream, L2 flushed (256 MiB write) between steps; max over ranks; seconds per LP for the whole job.
-* e2e   -- the same solve through the public C ABI taral_pdhg_solve() from host arrays: host scaling,
-  host-to-device upload of A, A^T and the vectors, the solve, the device-to-host download and the
-  original-space check, every step.
+* e2e   -- the same solve through the public C ABI taral_pdhg_solve() from host arrays: host transposes,
+  host-to-device upload of A, A^T and the vectors, scaling on the device, the solve, the device-to-host download
+  and the original-space check, every step.
 
+Once per run on rank 0 at N = 1, after the timed region (each can be skipped by its flag):
+* fp64      -- the same LP solved with FP64 iterates (the reference's precision): device time, iterations
+               against the reference's own FP64 count on this LP (--no-fp64);
+* family    -- the batched scenario family (512 refinery LPs of 4-48 periods) in one batched context against the
+               plain single-instance engine, every status, the independent FP64 check of all answers, and an FP64
+               objective oracle (this engine in FP64 to 1e-9 with a weak-duality certificate) on a stratified
+               sample plus the 48-period refinery LP (--no-family);
+* cpu_baseline -- one complete run of the reference's CPU PDHG (FP64, all host threads) to 1e-6 on the LP,
+               and the reference's CPU IPM and dual simplex on a small planted LP (--no-cpu-baseline).
 Also reported: the roofline of the dominant kernel (mean CUDA-event duration of the row-phase and column-phase
 kernels launched one at a time on the engine stream, algorithmic bytes per launch, against the measured HBM
-copy bandwidth) beside the random-gather floor measured in the same run, the reference's own CPU PDHG timed on a
-bounded sample on this host (and its CPU IPM and dual simplex on a small planted LP), SM clocks sampled during the
-timed region, and the number of engine kernels launched in it.
+copy bandwidth) beside the random-gather floor measured in the same run, SM clocks sampled during the timed
+region, and the number of engine kernels launched in it.
 
   python bench.py [--gpus N] [--steps K] [--warmup W]        our engine
-  python bench.py --impl reference ...                       the reference CPU PDHG (oracle/_ref/pdhg), plus its GPU
-                                                             backend on the same LP (--no-reference-gpu skips it)
+  python bench.py --impl reference ...                       the reference's own PDHG (oracle/_ref/pdhg, built from
+                                                             its sources): complete FP64 solves of the LP on its GPU
+                                                             backend, and one complete run of its CPU backend
   python bench.py [--impl reference] --workload ledger       the reference's published workloads, FP64 (either arm)
   python bench.py --profile-blocks B                         ncu capture mode: B blocks of 64 steps, no report
-  python bench.py --workload family [--instances 512]        the batched scenario family against the plain engine
+  python bench.py --workload family [--instances 512]        the family block alone
   python bench.py --workload family --profile-blocks B       ncu capture mode of the batched engine (16 scenarios)
   python bench.py --workload warmstart [--train 512]         the learned warm start on the 24-period family
 """
@@ -50,7 +59,6 @@ if "LOCAL_RANK" in os.environ and "CUDA_VISIBLE_DEVICES" not in os.environ:
 WORKLOAD = dict(m=200_000, n=500_000, per_col=10, zipf=1.2, cap=2000, floor=5, tol=1e-6)
 WORKLOAD_NAME = "planted LP, Zipf rows: m=200000 n=500000 ~5M nnz (row lengths Zipf s=1.2, cap 2000), tol 1e-6"
 METRIC = "time-to-1e-6 rel KKT per LP"
-REF_SAMPLE_ITERS = 256
 
 
 def dist_max(v, dist, device="cuda"):
@@ -131,12 +139,11 @@ def ref_binary():
     return ROOT / "oracle" / "_ref" / "pdhg"
 
 
-def cpu_solvers(cap_s=120.0):
+def cpu_solvers(cap_s=120.0, with_engine=True):
     """The reference's own CPU dual simplex and IPM (single-threaded engines of `oracle/_ref/taral`, each capped at
     cap_s seconds) and this engine on the small planted LP (2,000 x 5,000, 5 nonzeros per column, seed 1), timed
     in this run on this host, with the objective errors against the planted optimum. A reported baseline only."""
     import lpgen
-    import pdhg
     taral = ROOT / "oracle" / "_ref" / "taral"
     if not taral.exists():
         return None
@@ -156,6 +163,9 @@ def cpu_solvers(cap_s=120.0):
                                "objective_rel_err": abs(rep["objective"] - lp.obj_star) / abs(lp.obj_star)}
             except (subprocess.SubprocessError, OSError, ValueError, KeyError) as e:
                 out[method] = {"s": time.perf_counter() - t0, "status": f"failed: {type(e).__name__}"}
+    if not with_engine:
+        return out
+    import pdhg
     for name, prec in (("gpu_pdhg_fp32", pdhg.FP32), ("gpu_pdhg_fp64", pdhg.FP64)):
         pdhg.solve(lp, tol=1e-6, precision=prec)  # untimed first call
         ts, r = [], None
@@ -187,35 +197,44 @@ def mps_file(lp):
     return f
 
 
-def run_reference_sample(lp, iters, threads):
-    """The reference CPU PDHG (--device cpu, FP64) on the model for `iters` iterations; per-iteration seconds."""
+def run_reference(lp, device, tol=1e-6, limit_s=900.0, threads=0, max_iter=None):
+    """One run of the reference binary (oracle/_ref/pdhg, FP64, built from the reference's sources) on the model:
+    its JSON report plus the wall time of the process, or {"status": "failed: ..."}."""
     f = mps_file(lp)
+    cmd = [str(ref_binary()), str(f), "--device", device, "--tol", str(tol), "--time-limit", str(limit_s)]
+    if device == "cpu":
+        cmd += ["--threads", str(threads or os.cpu_count() or 1)]
+    if max_iter:
+        cmd += ["--max-iter", str(max_iter)]
     with tempfile.TemporaryDirectory() as td:
         j = Path(td) / "r.json"
-        subprocess.run([str(ref_binary()), str(f), "--device", "cpu", "--threads", str(threads), "--tol", "1e-6",
-                        "--max-iter", str(iters), "--json", str(j)], check=True, stdout=subprocess.DEVNULL,
-                       timeout=1800)
-        rep = json.loads(j.read_text())
-    per_it = (rep["solve_s"] - rep["power_iter_s"]) / max(rep["iterations"], 1)
-    setup = rep["scale_s"] + rep["transfer_s"]
-    return per_it, setup, rep
-
-
-def run_reference_gpu(lp, limit_s=120.0):
-    """The reference's own GPU backend (oracle/_ref/pdhg --device gpu, its default FP64, built for sm_100a from its
-    sources) on the model to 1e-6, capped at limit_s: its JSON report, or {"status": "failed: ..."}."""
-    f = mps_file(lp)
-    with tempfile.TemporaryDirectory() as td:
-        j = Path(td) / "r.json"
+        t0 = time.perf_counter()
         try:
-            subprocess.run([str(ref_binary()), str(f), "--device", "gpu", "--tol", "1e-6", "--time-limit", str(limit_s),
-                            "--json", str(j)], check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL,
-                           timeout=limit_s + 300)
+            subprocess.run(cmd + ["--json", str(j)], check=True, stdout=subprocess.DEVNULL,
+                           stderr=subprocess.DEVNULL, timeout=limit_s + 300)
             rep = json.loads(j.read_text())
         except (subprocess.SubprocessError, OSError, ValueError) as e:
             return {"status": f"failed: {type(e).__name__}"}
-    return {k: rep.get(k) for k in ("status", "iterations", "restarts", "objective", "setup_s", "solve_s", "total_s",
-                                    "precision", "device")}
+        wall = time.perf_counter() - t0
+    out = {k: rep.get(k) for k in ("status", "iterations", "restarts", "objective", "setup_s", "solve_s", "total_s",
+                                   "power_iter_s", "precision", "device", "threads")}
+    out["process_wall_s"] = wall
+    return out
+
+
+def reference_cpu_complete(lp, threads):
+    """One complete run of the reference CPU PDHG (--device cpu, FP64, `threads` host threads) to 1e-6 on the LP,
+    measured (no projection), as a cpu_baseline dict."""
+    rep = run_reference(lp, "cpu", threads=threads, limit_s=1200.0)
+    if not str(rep.get("status", "")).startswith("near"):
+        return {"value": None, "unit": "s", "cores": threads, "kind": "reference", "complete_runs": 0,
+                "sample": f"one run of the reference CPU PDHG (FP64, {threads} threads) to 1e-6: {rep.get('status')}"}
+    return {"value": rep["solve_s"], "unit": "s", "cores": threads, "kind": "reference", "complete_runs": 1,
+            "total_s": rep["total_s"], "iterations": rep["iterations"], "status": rep["status"],
+            "objective": rep["objective"],
+            "sample": f"one complete run of the reference CPU PDHG (oracle/_ref/pdhg --device cpu --threads {threads}, "
+                      f"FP64) on this LP to 1e-6 rel KKT, measured: value = its solve time, total_s = with its MPS "
+                      f"parse and scaling"}
 
 
 REF_BENCH_LP = ROOT / "tests" / "golden" / "reference_bench_lp.json"
@@ -230,7 +249,20 @@ def fp64_iterations(lp):
     return d["iterations"], d["status"]
 
 
+def lp_config(m, n, nnz):
+    """The `config` object of both arms (the same workload, so the same keys and values)."""
+    return {"workload": WORKLOAD_NAME, "m": m, "n": n, "nnz": nnz, "tol": WORKLOAD["tol"], "seed": "rank (0 at N=1)",
+            "parallelism": "replicas (one LP per GPU)",
+            "l2": "inputs larger than L2 (~190 MB of matrices and vectors); L2 flushed (256 MiB write) between steps "
+                  "of this engine, every step of the reference re-reads its model and uploads it anew"}
+
+
 def reference_arm(args, rank, world):
+    """The reference's own implementation of the path, unmodified, through its public interface (the `pdhg` CLI on
+    an MPS file): `value` is the median solve time of complete FP64 runs of its GPU backend to 1e-6 on this LP (W
+    untimed runs, then K timed), `e2e` the median of the same runs' totals (MPS parse, scaling, upload, solve).
+    Its FP32 mode does not reach 1e-6 on this LP (time_limit), so FP64 is the reference's configuration here.
+    `cpu_baseline`: one complete run of its CPU backend on all host threads, measured."""
     if rank != 0:
         return
     threads = os.cpu_count() or 1
@@ -238,29 +270,37 @@ def reference_arm(args, rank, world):
     if not ref_binary().exists():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/pdhg was not built (make -C oracle ref)"}))
         return
-    if not REF_BENCH_LP.exists():
-        print(json.dumps({"impl": "reference", "unavailable": "tests/golden/reference_bench_lp.json is missing"}))
-        return
-    n_it, st = fp64_iterations(lp)
-    vals = []
+    n_it, _ = fp64_iterations(lp) if REF_BENCH_LP.exists() else (None, None)
+    runs = []
     for s in range(args.warmup + args.steps):
-        per_it, setup, rep = run_reference_sample(lp, REF_SAMPLE_ITERS, threads)
+        rep = run_reference(lp, "gpu", limit_s=600.0)
+        print(json.dumps({"reference_gpu_run": s, **rep}), file=sys.stderr, flush=True)
         if s >= args.warmup:
-            vals.append(setup + rep["power_iter_s"] + per_it * n_it)
-    v = statistics.median(vals)
-    sample = (f"{REF_SAMPLE_ITERS} iterations of the reference CPU PDHG (--device cpu --threads {threads}, FP64) per "
-              f"step; time-to-1e-6 = scale + power iteration + per-iteration time x {n_it} iterations (the FP64 "
-              f"iteration count to 1e-6 on this LP)")
+            runs.append(rep)
+    ok = [r for r in runs if r.get("solve_s") is not None]
+    if not ok:
+        print(json.dumps({"impl": "reference", "unavailable": "the reference GPU backend failed: " +
+                          str(runs[0].get("status") if runs else "no run")}))
+        return
+    v = statistics.median(r["solve_s"] for r in ok)
+    e2e = statistics.median(r["total_s"] for r in ok)
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak",
-            "vs_baseline": None, "dtype": "fp64", "data": "synthetic",
-            "config": {"workload": WORKLOAD_NAME, "seed": 0, "tol": WORKLOAD["tol"], "parallelism": "cpu threads",
-                       "l2": "n/a (CPU)", "fp64_iterations_to_tol": n_it, "fp64_status": st},
-            "cpu_baseline": {"value": v, "unit": "s", "cores": threads, "kind": "reference", "sample": sample},
-            "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    if not args.no_reference_gpu:  # beside the CPU arm: the reference's GPU backend on the same LP and GPU, untimed here
-        line["gpu_backend"] = {"what": "the reference's own GPU PDHG (--device gpu, FP64: its FP32 mode does not reach "
-                                       "1e-6 on this LP) on the same LP, one run", **run_reference_gpu(lp)}
+            "vs_baseline": None, "dtype": "fp64", "data": "synthetic", "config": lp_config(lp.m, lp.n, lp.nnz),
+            "run": {"what": "oracle/_ref/pdhg --device gpu --tol 1e-6 (FP64, its default) per step, the reference's "
+                            "stock CLI on the LP written as MPS",
+                    "statuses": [r.get("status") for r in runs], "iterations": [r.get("iterations") for r in runs],
+                    "reference_fp64_iterations_on_cpu": n_it, "restarts": ok[-1].get("restarts"),
+                    "objective": ok[-1].get("objective"),
+                    "objective_rel_err_vs_planted": abs(ok[-1]["objective"] - lp.obj_star) / abs(lp.obj_star),
+                    "solve_s": [r.get("solve_s") for r in runs], "total_s": [r.get("total_s") for r in runs],
+                    "process_wall_s": [r.get("process_wall_s") for r in runs], "device": ok[-1].get("device")},
+            "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
+                    "what": "median total_s of the timed runs: the reference's own clock from reading the MPS file to "
+                            "its answer (parse, host scaling, upload, solve, check); copies happen inside its process"}}
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = reference_cpu_complete(lp, threads)
+        line["cpu_baseline"]["solvers_small_lp"] = cpu_solvers(with_engine=False)
     print(json.dumps(line))
 
 
@@ -378,27 +418,23 @@ def our_arm(args, rank, world, dist):
     floor = gather_floor(nnz) if rank == 0 and (m, n) == (200_000, 500_000) else None
 
     if rank == 0:
+        once = world == 1  # the once-per-run blocks: rank 0 at N = 1 only
+        fp64 = fp64_block(lp) if once and not args.no_fp64 else None
+        family = family_block(args) if once and not args.no_family else None
         cpu = None
-        if ref_binary().exists() and REF_BENCH_LP.exists() and world == 1 and not args.no_cpu_baseline:
-            n_it, _ = fp64_iterations(lp)
-            threads = os.cpu_count() or 1
-            per_it, setup, rep = run_reference_sample(lp, REF_SAMPLE_ITERS, threads)
-            cpu = {"value": setup + rep["power_iter_s"] + per_it * n_it, "unit": "s", "cores": threads,
-                   "kind": "reference",
-                   "sample": f"{REF_SAMPLE_ITERS} iterations of the reference CPU PDHG (FP64, {threads} threads) "
-                             f"on this LP, projected to the {n_it} FP64 iterations to 1e-6 plus its setup"}
-        solvers = cpu_solvers() if cpu is not None else None  # the reference CPU solvers on the small LP
+        if once and not args.no_cpu_baseline and ref_binary().exists():
+            cpu = reference_cpu_complete(lp, os.cpu_count() or 1)
+            cpu["solvers_small_lp"] = cpu_solvers()
         r0 = outs[-1]
         line = {
             "metric": METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": value * 1e3 * world, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
-            "config": {"workload": WORKLOAD_NAME, "m": m, "n": n, "nnz": nnz, "tol": tol, "seed": "rank",
-                       "precision": "fp32 matrix/iterates, fp64 averages/KKT/restarts",
-                       "parallelism": f"replicas x{world}", "l2": "flushed between steps (256 MiB write)",
-                       "iterations": its, "restarts": r0["restarts"], "status": r0["status"],
-                       "rel_kkt": max(r0["rel_primal"], r0["rel_dual"], r0["rel_gap"]),
-                       "objective_rel_err_vs_planted": abs(e2e_out[-1]["objective"] - lp.obj_star) / abs(lp.obj_star)},
+            "config": lp_config(m, n, nnz),
+            "run": {"precision": "fp32 matrix/iterates, fp64 averages/KKT/restarts", "iterations": its,
+                    "restarts": r0["restarts"], "status": r0["status"],
+                    "rel_kkt": max(r0["rel_primal"], r0["rel_dual"], r0["rel_gap"]),
+                    "objective_rel_err_vs_planted": abs(e2e_out[-1]["objective"] - lp.obj_star) / abs(lp.obj_star)},
             "e2e": {"value": e2e_value, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "phases_s": {k: e2e_out[-1][k] for k in ("scale_s", "device_init_s", "transfer_s", "solve_s")},
                     "steps_s": e2e_steps, "warmup_calls": 1},
@@ -413,11 +449,33 @@ def our_arm(args, rank, world, dist):
                              "col_frac": floor[m] / (col_ms * 1e3) if m in floor else None,
                              "source": "bin/gather_floor in this run: the same count of random 4-byte gathers "
                                        "with their index/value stream, L2 flushed before each launch"}},
-            "cpu_baseline": cpu if cpu is None or solvers is None else {**cpu, "solvers_small_lp": solvers},
+            "fp64": fp64,
+            "family": family,
+            "cpu_baseline": cpu,
             "gpu_launches": launches,
             "clocks": clk,
         }
         print(json.dumps(line))
+
+
+def fp64_block(lp):
+    """The bench LP with FP64 iterates (the reference's precision): one solve through taral_pdhg_solve from host
+    arrays (end to end, like `e2e`; it also loads the FP64 kernels), then one on a resident context, timed with CUDA
+    events like `value`."""
+    import pdhg
+    tol = WORKLOAD["tol"]
+    t0 = time.perf_counter()
+    r_e2e, _, _ = pdhg.solve(lp, tol=tol, precision=pdhg.FP64)
+    e2e_s = time.perf_counter() - t0
+    eng = pdhg.Engine.from_model(lp, precision=pdhg.FP64)
+    r, _, _ = eng.solve(eng.bnorm, eng.cnorm, tol=tol, want_point=False)
+    eng.close()
+    n_it, _ = fp64_iterations(lp) if REF_BENCH_LP.exists() else (None, None)
+    return {"device_s": r["device_s"], "e2e_s": e2e_s, "iterations": r["iterations"], "restarts": r["restarts"],
+            "status": r["status"], "reference_fp64_iterations": n_it,
+            "iterations_equal_reference": None if n_it is None else (r["iterations"] == n_it == r_e2e["iterations"]),
+            "objective": r_e2e["objective"],
+            "objective_rel_err_vs_planted": abs(r_e2e["objective"] - lp.obj_star) / abs(lp.obj_star)}
 
 
 # The reference's own published GPU workloads (gpu/gen_lp.py models, reproduced byte for byte by lpgen), FP64 to
@@ -437,7 +495,7 @@ def ledger_arm(args, reference):
         lp = make(lpgen)
         row = {"ledger_iterations": ledger_it, "published_solve_s_rtx5050": published_s}
         if reference:
-            row["reference_gpu_fp64"] = run_reference_gpu(lp, limit_s=600.0)
+            row["reference_gpu_fp64"] = run_reference(lp, "gpu", limit_s=600.0)
         else:
             import pdhg
             for tag, prec in (("fp64", pdhg.FP64), ("fp32", pdhg.FP32)):
@@ -480,11 +538,29 @@ def family_profile(args):
     print("profiled", len(res), "scenarios,", res[0]["iterations"], "iterations")
 
 
-def family_arm(args):
-    """All scenarios in one batched context (FP32 iterates, FP64 per-instance restart state) against the plain
-    single-instance FP32 engine on a stratified sample of them; the plain per-LP time of the whole family is the
-    least-squares line in the number of periods through the sample, evaluated at every scenario's period count."""
+def fp64_oracle(lp, tol=1e-9, time_limit=300.0):
+    """The FP64 objective oracle of a refinery LP (only a feasible point is planted there): this engine with FP64
+    iterates to `tol` relative KKT, and the weak-duality bound of its dual vector from the independent device check
+    (the reference checker's rule): objective, certified relative gap between them, status and time."""
+    import pdhg
+    t0 = time.perf_counter()
+    r, x, y = pdhg.solve(lp, tol=tol, precision=pdhg.FP64, time_limit=time_limit)
+    dt = time.perf_counter() - t0
+    c = pdhg.check_models([lp], [x], [y])[0]
+    lb = c["dual_bound"] if c["dual_bound"] is not None else c["dual_obj_loose"]
+    return {"objective": r["objective"], "status": r["status"], "iterations": r["iterations"], "seconds": dt,
+            "dual_bound": lb, "strict_bound": c["dual_bound"] is not None,
+            "certified_gap_rel": None if lb is None else abs(r["objective"] - lb) / max(1.0, abs(r["objective"]))}
+
+
+def family_block(args):
+    """The batched scenario family: all scenarios in one batched context (FP32 iterates, FP64 per-instance restart
+    state) against the plain single-instance FP32 engine on a stratified sample (fastest of 3 runs each; the plain
+    per-LP time of the whole family is the least-squares line in the period count through the sample, evaluated at
+    every scenario's period count), the independent FP64 check of every answer, and the FP64 objective oracle on a
+    stratified sample and on the 48-period refinery LP."""
     import numpy as np
+    import lpgen
     import pdhg
     tol = WORKLOAD["tol"]
     t0 = time.perf_counter()
@@ -496,15 +572,14 @@ def family_arm(args):
     batch_s = time.perf_counter() - t0
     info = b.info()
     b.close()
-    # independent FP64 check of every answer on its original model, on the device (not part of the timed solve)
     t0 = time.perf_counter()
     chk = pdhg.check_models(lps, bx, by)
     check_s = time.perf_counter() - t0
     del bx, by
     order = np.argsort(periods, kind="stable")
     pick = order[np.linspace(0, len(order) - 1, min(args.sample, len(order))).round().astype(int)]
-    plain_t, plain_T, obj_diff = [], [], []
-    for i in pick:  # each sample solved three times, the fastest kept (host hiccups of a shared box excluded)
+    plain_t, plain_T, obj_diff, plain_it = [], [], [], []
+    for i in pick:
         dt = float("inf")
         for _ in range(3):
             t0 = time.perf_counter()
@@ -512,28 +587,45 @@ def family_arm(args):
             dt = min(dt, time.perf_counter() - t0)
         plain_t.append(dt)
         plain_T.append(int(periods[i]))
+        plain_it.append(int(r["iterations"]))
         obj_diff.append(abs(r["objective"] - res[i]["objective"]) / max(1.0, abs(r["objective"])))
-        print(f"plain T={periods[i]} {plain_t[-1]:.3f}s it={r['iterations']} batched it={res[i]['iterations']} "
-              f"(scale {r['scale_s']:.3f} init {r['device_init_s']:.3f} transfer {r['transfer_s']:.3f} "
-              f"solve {r['solve_s']:.3f} device {r['device_s']:.3f})", file=sys.stderr, flush=True)
     slope, icpt = np.polyfit(np.array(plain_T, float), np.array(plain_t), 1)
     plain_per_lp = float(np.mean(np.maximum(slope * periods + icpt, 0.0)))
+    # FP64 objective oracle: a stratified sample of the family, then the 48-period refinery LP itself
+    oracle_rows = []
+    for i in order[np.linspace(0, len(order) - 1, min(args.oracle_sample, len(order))).round().astype(int)]:
+        o = fp64_oracle(lps[i])
+        o.update({"scenario": int(i), "periods": int(periods[i]), "batched_objective": res[i]["objective"],
+                  "batched_rel_diff": abs(res[i]["objective"] - o["objective"]) / max(1.0, abs(o["objective"]))})
+        oracle_rows.append(o)
+        print("fp64 oracle", json.dumps(o), file=sys.stderr, flush=True)
+    lp48 = lpgen.RefineryBase(48, seed=7).instance(48)
+    t0 = time.perf_counter()
+    r48, _, _ = pdhg.solve(lp48, tol=tol, precision=pdhg.FP32, time_limit=600)
+    s48 = time.perf_counter() - t0
+    o48 = fp64_oracle(lp48)
+    refinery48 = {"m": lp48.m, "n": lp48.n, "nnz": lp48.nnz, "fp32_status": r48["status"],
+                  "fp32_iterations": r48["iterations"], "fp32_e2e_s": s48, "fp32_objective": r48["objective"],
+                  "fp64_oracle": o48,
+                  "fp32_rel_diff": abs(r48["objective"] - o48["objective"]) / max(1.0, abs(o48["objective"]))}
     k = len(lps)
     its = [r["iterations"] for r in res]
-    line = {"metric": "time-to-1e-6 rel KKT per LP (batched scenario family)", "value": batch_s / k, "unit": "s",
-            "n_gpus": 1, "higher_is_better": False, "dtype": "fp32", "data": "synthetic",
-            "config": {"workload": f"refinery scenario family: {k} LPs of 4-48 periods (1,500 rows x 4,000 columns "
-                                   f"per period), prices and capacities x U(0.8,1.2), tol {tol}",
-                       "rows_total": int(sum(lp.m for lp in lps)), "cols_total": int(sum(lp.n for lp in lps)),
-                       "nnz_total": info["nnz_total"], "nnz_stored": info["nnz_stored"],
-                       "distinct_matrices": info["distinct_matrices"], "device_mem_bytes": info["device_mem_bytes"]},
+    statuses = {}
+    for r in res:
+        statuses[r["status"]] = statuses.get(r["status"], 0) + 1
+    return {"metric": "time-to-1e-6 rel KKT per LP, batched scenario family vs the plain engine",
+            "workload": f"refinery scenario family: {k} LPs of 4-48 periods (1,500 rows x 4,000 columns per period), "
+                        f"prices and capacities x U(0.8,1.2), tol {tol}, FP32 iterates",
+            "rows_total": int(sum(lp.m for lp in lps)), "cols_total": int(sum(lp.n for lp in lps)),
+            "nnz_total": info["nnz_total"], "nnz_stored": info["nnz_stored"],
+            "distinct_matrices": info["distinct_matrices"], "device_mem_bytes": info["device_mem_bytes"],
             "batched": {"wall_s": batch_s, "per_lp_s": batch_s / k, "device_s": res[0]["device_s"],
-                        "near_optimal": sum(r["status"] == "near_optimal" for r in res),
-                        "iterations_mean": float(np.mean(its)), "iterations_max": int(max(its))},
-            "plain_single_instance": {"per_lp_s_fit": plain_per_lp, "sample": len(pick),
-                                      "sample_periods": plain_T, "sample_s": plain_t,
+                        "statuses": statuses, "iterations_mean": float(np.mean(its)), "iterations_max": int(max(its))},
+            "plain_single_instance": {"per_lp_s_fit": plain_per_lp, "sample": len(pick), "sample_periods": plain_T,
+                                      "sample_s": plain_t, "sample_iterations": plain_it,
                                       "fit_s_per_period": float(slope), "fit_intercept_s": float(icpt)},
             "speedup_per_lp": plain_per_lp / (batch_s / k),
+            "objective_max_rel_diff_batched_vs_plain": float(max(obj_diff)),
             "independent_check": {"seconds": check_s,
                                   "max_row_violation_rel": max(c["row_violation_rel"] for c in chk),
                                   "max_bound_violation": max(c["bound_violation"] for c in chk),
@@ -541,8 +633,17 @@ def family_arm(args):
                                   "strict_dual_bounds": sum(c["dual_bound"] is not None for c in chk),
                                   "max_objective_diff_vs_solver": max(abs(c["objective"] - r["objective"]) /
                                                                       max(1.0, abs(r["objective"])) for c, r in zip(chk, res))},
-            "objective_max_rel_diff_batched_vs_plain": float(max(obj_diff)), "generate_s": gen_s}
-    print(json.dumps(line))
+            "fp64_oracle": {"what": "this engine in FP64 to 1e-9 rel KKT; certified_gap_rel = |objective - weak-duality "
+                                    "bound of its y| / max(1, |objective|) from the independent check",
+                            "sample": oracle_rows,
+                            "max_batched_rel_diff": max(o["batched_rel_diff"] for o in oracle_rows) if oracle_rows else None,
+                            "max_certified_gap_rel": max((o["certified_gap_rel"] or 0.0) for o in oracle_rows) if oracle_rows else None},
+            "refinery_48_periods": refinery48,
+            "generate_s": gen_s}
+
+
+def family_arm(args):
+    print(json.dumps(family_block(args)))
 
 
 def warmstart_arm(args):
@@ -595,8 +696,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--profile-blocks", type=int, default=0)
-    ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-reference-gpu", action="store_true", help="reference arm: skip its GPU backend run")
+    ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the complete CPU run of the reference")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 run of the bench LP")
+    ap.add_argument("--no-family", action="store_true", help="skip the batched family block")
+    ap.add_argument("--oracle-sample", type=int, default=4, help="family scenarios given the FP64 objective oracle")
     ap.add_argument("--workload", choices=["lp", "family", "warmstart", "ledger"], default="lp",
                     help="lp: the single large LP (the bench line); family: the batched scenario family; "
                          "warmstart: the learned warm start on the 24-period family; ledger: the reference's "

@@ -39,7 +39,8 @@ enum taral_status {
     TARAL_ERR_UNSUPPORTED = -4, /* integer or quadratic model (gpu/pdhg_input.hpp:7-17) */
     TARAL_ERR_PARSE = -5,       /* MPS file could not be read */
     TARAL_ERR_STATE = -6,       /* call out of order (e.g. iterate before start) */
-    TARAL_ERR_NO_DEVICE = -7    /* no CUDA device, or not an sm_100 part */
+    TARAL_ERR_NO_DEVICE = -7,   /* no CUDA device, or not an sm_100 part */
+    TARAL_ERR_CANCELLED = -8    /* the solve stopped on a cancel request (taral_batch_cancel); outputs are filled */
 };
 
 /* Arithmetic of the iteration. FP64: everything in double (the reference's default).
@@ -130,7 +131,7 @@ typedef struct {
 } taral_options;
 
 enum taral_solve_status { TARAL_NEAR_OPTIMAL = 0, TARAL_ITERATION_LIMIT = 1, TARAL_TIME_LIMIT = 2,
-                          TARAL_NUMERICAL_FAILURE = 3 };
+                          TARAL_NUMERICAL_FAILURE = 3, TARAL_CANCELLED = 4 /* batch: stopped by taral_batch_cancel */ };
 
 /* Outcome (gpu/pdhg.cu:752-759) and the figures finish() prints (gpu/pdhg.cu:866-897). */
 typedef struct {
@@ -180,6 +181,12 @@ int pdhg_solve_ctx(pdhg_ctx* ctx, double bnorm, double cnorm, const taral_option
  * column-phase kernel (A^T z + primal step), each run bracketed by CUDA events on the context stream. Returns the
  * mean milliseconds per launch of each. Leaves the iterate in an unspecified state: start again before solving. */
 int pdhg_profile_phases(pdhg_ctx* ctx, int reps, double* row_ms, double* col_ms);
+/* Inspection of the scaled problem a context holds (the reference's Scaled, gpu/pdhg.cu:72-78, which it keeps on the
+ * host): Dr (m), Dc (n), the values of A_s = diag(Dr) A diag(Dc) (nnz; rows in the model's order, each row's entries
+ * in column order, explicit zeros of the model dropped) and of A_s^T (nnz, its rows in column order, entries in row
+ * order), copied from the device and widened to double (an FP32 context holds them narrowed to float). Any pointer
+ * may be NULL. For checking the device-side set-up against a host computation of the same scaling. */
+int pdhg_scaled_problem(pdhg_ctx* ctx, double* Dr, double* Dc, double* A_val, double* AT_val);
 
 /* ------------------------------------------------------------------------------------------------------------
  * 3. Problem format. Replaces read_mps (src/taral.hpp:48, src/mps.cpp:388-399): free format first, fixed
@@ -228,11 +235,23 @@ int taral_batch_create(const taral_model* models, int count, const taral_options
  * and device_s are the whole batch's). x_out[i] (n_i) / y_out[i] (m_i) may be NULL, as may x_out / y_out. */
 int taral_batch_solve(taral_batch* b, const double* const* x0, const double* const* y0, const double* w0,
                       taral_outcome* outs, double* const* x_out, double* const* y_out);
+/* Ask a running taral_batch_solve on b to stop; callable from any host thread (the only call that may overlap a
+ * solve on the same batch). The flag lives in pinned host memory that the device's decision kernel reads after every
+ * block of eval_freq iterations: every instance still running then stops with status TARAL_CANCELLED, its best
+ * point so far is downloaded and checked as usual, and taral_batch_solve returns TARAL_ERR_CANCELLED. A request made
+ * while no solve runs applies to the next solve; a solve clears the flag when it returns. */
+int taral_batch_cancel(taral_batch* b);
 /* Distinct stored matrices, device bytes, nonzeros stored and nonzeros over all instances. */
 int taral_batch_info(const taral_batch* b, int* distinct_matrices, size_t* device_mem, int64_t* nnz_stored,
                      int64_t* nnz_total);
 const char* taral_batch_last_error(const taral_batch* b);
 void taral_batch_destroy(taral_batch* b);
+
+/* Fault-injection hook for tests (no counterpart in the reference, whose CHECK macro exits the process on any CUDA
+ * error, gpu/pdhg.cu:36-43): from now on, a context or batch whose device allocations would exceed `bytes` in total
+ * fails as if the device were out of memory, and its create call returns TARAL_ERR_ALLOC after releasing what it
+ * had allocated. 0 (the default) removes the limit. Process-wide; set it while no create call runs. */
+void taral_set_device_alloc_limit(size_t bytes);
 
 /* ------------------------------------------------------------------------------------------------------------
  * 7. Learned warm start: an MLP (in -> hidden x depth with GELU -> out) trained and evaluated with this library's
@@ -262,6 +281,13 @@ int taral_gemm_bf16(int M, int N, int K, int ta, int tb, const void* A, const vo
  * A (M x K) and Bt (N x K) bf16, row-major, 16-byte aligned, K a multiple of 8. err: a device int that is set to 1
  * if a completion wait gave up (C is then undefined); it is never cleared here. Asynchronous on `stream`. */
 int taral_gemm_bf16_tc(int M, int N, int K, const void* A, const void* Bt, float* C, int* err, void* stream);
+/* The general tcgen05 GEMM behind the MLP's three GEMMs: C (M x N, f32, row stride ldc) = sum_k A(m, k) B(n, k) with
+ * bf16 operands brought in by TMA. a_mn = 0: A stored [M][lda] (K contiguous); a_mn = 1: A stored [K][lda] (M
+ * contiguous); likewise b_mn for B with N. lda and ldb multiples of 8, A and B 16-byte aligned. slices > 1 splits K
+ * into that many slices whose partials (in `workspace`, slices * M * ldc floats) are summed in slice order. err as
+ * for taral_gemm_bf16_tc. Asynchronous on `stream`. */
+int taral_gemm_bf16_umma(int M, int N, int K, const void* A, int lda, int a_mn, const void* B, int ldb, int b_mn,
+                         float* C, int ldc, int slices, float* workspace, int* err, void* stream);
 
 /* ------------------------------------------------------------------------------------------------------------
  * 6. KKT evaluation without device allocation. No counterpart in the reference: it is an addition for callers

@@ -264,11 +264,12 @@ __global__ void k_eval_finish(int ninst, const int2* __restrict__ where, const i
 }
 
 // The schedule's decision after a block (schedule.hpp, judge_block) for every running instance, one thread each.
-// The deadline is compared with %globaltimer (0: none). rflag[i]: where instance i restarts (RestartTo).
+// External stops: the host's cancel flag (pinned host memory, read through its device mapping) and the deadline,
+// compared with %globaltimer (0: none). rflag[i]: where instance i restarts (RestartTo).
 template <class T>
 __global__ void k_decide(int ninst, InstState* st, const double* __restrict__ kc_all, const double* __restrict__ ka_all,
                          double* par, int* running, int* rflag, double tol, double row_rel, long long max_iter,
-                         const unsigned long long* deadline) {
+                         const unsigned long long* deadline, const volatile int* cancel) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= ninst) return;
     rflag[i] = kNoRestart;
@@ -277,7 +278,8 @@ __global__ void k_decide(int ninst, InstState* st, const double* __restrict__ kc
     unsigned long long now;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
     const StopRule rule{tol, row_rel, s.bnorm, s.cnorm, max_iter};
-    const BlockDecision d = judge_block(s.sch, kc_all + 10 * i, ka_all + 10 * i, rule, *deadline && now > *deadline);
+    const int stop = *cancel ? int(TARAL_CANCELLED) : (*deadline && now > *deadline) ? int(TARAL_TIME_LIMIT) : -1;
+    const BlockDecision d = judge_block(s.sch, kc_all + 10 * i, ka_all + 10 * i, rule, stop);
     s.best_p = d.best.primal, s.best_d = d.best.dual, s.best_g = d.best.gap, s.avg_final = d.average_better;
     if (d.status >= 0) {
         s.status = d.status, s.running = 0, running[i] = 0;
@@ -463,9 +465,10 @@ uint64_t fnv(const void* p, size_t n, uint64_t h) {  // FNV-1a over 8-byte words
 
 struct BatchBase {
     virtual ~BatchBase() = default;
-    virtual void solve(const double* const* x0, const double* const* y0, const double* w0, taral_outcome* outs,
-                       double* const* xo,
-                       double* const* yo) = 0;
+    // Returns TARAL_OK, or TARAL_ERR_CANCELLED when a cancel request stopped some instance.
+    virtual int solve(const double* const* x0, const double* const* y0, const double* w0, taral_outcome* outs,
+                      double* const* xo, double* const* yo) = 0;
+    virtual void cancel() = 0;  // any host thread, also during solve()
     std::string err;
     int distinct = 0;
     size_t mem_used = 0;
@@ -516,6 +519,8 @@ struct Batch final : BatchBase {
     InstState* st = nullptr;
     unsigned long long* d_deadline = nullptr;
     int *running = nullptr, *rflag = nullptr, *pactive = nullptr, *count = nullptr, *h_count = nullptr;
+    int* h_cancel = nullptr;        // pinned, mapped host memory: the cancel request (0 / 1)
+    const int* d_cancel = nullptr;  // its device address
     cudaStream_t s = nullptr;
     cudaGraphExec_t graph = nullptr;
     std::vector<void*> allocs;
@@ -524,6 +529,8 @@ struct Batch final : BatchBase {
     U* alloc(size_t n) {  // stream-ordered, from the device's memory pool (keep_pool_memory)
         void* p = nullptr;
         const size_t bytes = std::max<size_t>(n, 1) * sizeof(U);
+        if (!alloc_allowed(alloc_bytes, bytes))
+            throw BatchError{"cudaMalloc: the device allocation limit (taral_set_device_alloc_limit) is reached"};
         cudaError_t e = cudaMallocAsync(&p, bytes, s);
         if (e != cudaSuccess) throw BatchError{std::string("cudaMalloc: ") + cudaGetErrorString(e)};
         allocs.push_back(p);
@@ -543,6 +550,7 @@ struct Batch final : BatchBase {
         for (void* p : allocs) cudaFreeAsync(p, s);
         if (s) cudaStreamSynchronize(s);
         if (h_count) cudaFreeHost(h_count);
+        if (h_cancel) cudaFreeHost(h_cancel);
         if (s) cudaStreamDestroy(s);
     }
 
@@ -810,6 +818,11 @@ struct Batch final : BatchBase {
         running = alloc<int>(count), rflag = alloc<int>(count), pactive = alloc<int>(count), this->count = alloc<int>(1);
         d_deadline = alloc<unsigned long long>(1);
         BK(cudaMallocHost(&h_count, sizeof(int)));
+        BK(cudaHostAlloc(reinterpret_cast<void**>(&h_cancel), sizeof(int), cudaHostAllocMapped));
+        __atomic_store_n(h_cancel, 0, __ATOMIC_SEQ_CST);
+        void* dc = nullptr;
+        BK(cudaHostGetDevicePointer(&dc, h_cancel, 0));
+        d_cancel = static_cast<const int*>(dc);
         BK(cudaStreamSynchronize(s));
         mem_used = alloc_bytes;
         nnz_total = 0;
@@ -1014,7 +1027,7 @@ struct Batch final : BatchBase {
         eval_into(kkt, false, running);
         eval_into(kkt + 10 * size_t(ninst), true, running);
         k_decide<T><<<g, 256, 0, s>>>(ninst, st, kkt, kkt + 10 * size_t(ninst), par, running, rflag, opt.tol,
-                                      opt.row_rel, (long long)opt.max_iter, d_deadline);
+                                      opt.row_rel, (long long)opt.max_iter, d_deadline, d_cancel);
         if (nT) k_pack_restart<T><<<nT, kThreads, 0, s>>>(T_ev, Te_ev, slot_inst, rflag, st, x, xs, xlast);
         if (nA) k_pack_restart<T><<<nA, kThreads, 0, s>>>(A_ev, Ae_ev, slot_inst, rflag, st, z, zs, zlast);
         products(rflag);
@@ -1022,8 +1035,12 @@ struct Batch final : BatchBase {
         launches += 7;
     }
 
-    void solve(const double* const* x0, const double* const* y0, const double* w0, taral_outcome* outs,
-               double* const* xo, double* const* yo) override {
+    void cancel() override {
+        if (h_cancel) __atomic_store_n(h_cancel, 1, __ATOMIC_SEQ_CST);
+    }
+
+    int solve(const double* const* x0, const double* const* y0, const double* w0, taral_outcome* outs,
+              double* const* xo, double* const* yo) override {
         auto t0 = Clock::now();
         restore_lists();  // a previous solve may have left the lists compacted
         cudaEvent_t e0, e1;
@@ -1125,15 +1142,21 @@ struct Batch final : BatchBase {
         const bool trace = std::getenv("TARAL_TRACE") != nullptr;
         int live_lists = ninst;  // running instances when the lists were last built
         std::vector<int> live(static_cast<size_t>(ninst));
+        // One graph launch runs `per_launch` blocks of eval_freq iterations (TARAL_BATCH_BLOCKS, default 4): the
+        // decisions, restarts, the cancel flag and the deadline are all taken on the device after every block, and
+        // the kernels of stopped instances return at once, so the host only reads the running count (and compacts
+        // the iteration lists) between launches.
+        const char* pb = std::getenv("TARAL_BATCH_BLOCKS");
+        const int per_launch = std::max(1, std::min(64, pb ? std::atoi(pb) : 4));
         for (;;) {
-            int steps = int(std::min<int64_t>(freq, opt.max_iter - it));
-            if (steps <= 0) break;
-            if (steps == freq && opt.graph) {
+            const int64_t left = opt.max_iter - it;
+            if (left <= 0) break;
+            if (opt.graph && left >= int64_t(freq) * per_launch) {
                 if (!graph) {
                     cudaGraph_t gr;
                     int64_t before = launches;
                     BK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-                    block(steps);
+                    for (int q = 0; q < per_launch; ++q) block(freq);
                     BK(cudaStreamEndCapture(s, &gr));
                     BK(cudaGraphInstantiate(&graph, gr, 0));
                     BK(cudaGraphDestroy(gr));
@@ -1141,10 +1164,12 @@ struct Batch final : BatchBase {
                 }
                 BK(cudaGraphLaunch(graph, s));
                 launches += per_graph;
+                it += int64_t(freq) * per_launch;
             } else {
+                const int steps = int(std::min<int64_t>(freq, left));
                 block(steps);
+                it += steps;
             }
-            it += steps;
             BK(cudaMemcpyAsync(h_count, count, sizeof(int), cudaMemcpyDeviceToHost, s));
             BK(cudaStreamSynchronize(s));
             if (trace) std::fprintf(stderr, "batch block it=%lld running=%d t=%.4f\n", (long long)it, *h_count, since(t0));
@@ -1206,6 +1231,10 @@ struct Batch final : BatchBase {
                 for (int i = next++; i < ninst; i = next++) finish_one(i);
             });
         for (auto& th : pool) th.join();
+        __atomic_store_n(h_cancel, 0, __ATOMIC_SEQ_CST);  // a request applies to one solve
+        for (int i = 0; i < ninst; ++i)
+            if (fin[size_t(i)].status == TARAL_CANCELLED) return TARAL_ERR_CANCELLED;
+        return TARAL_OK;
     }
     int64_t per_graph = 0;
 };
@@ -1256,13 +1285,18 @@ extern "C" int taral_batch_solve(taral_batch* h, const double* const* x0, const 
                                  const double* w0, taral_outcome* outs, double* const* x_out, double* const* y_out) {
     if (!h || !outs) return TARAL_ERR_INPUT;
     try {
-        h->b->solve(x0, y0, w0, outs, x_out, y_out);
+        return h->b->solve(x0, y0, w0, outs, x_out, y_out);
     } catch (const taral::BatchError& e) {
         h->b->err = e.msg;
         return TARAL_ERR_CUDA;
     } catch (const std::bad_alloc&) {
         return TARAL_ERR_ALLOC;
     }
+}
+
+extern "C" int taral_batch_cancel(taral_batch* h) {
+    if (!h || !h->b) return TARAL_ERR_INPUT;
+    h->b->cancel();
     return TARAL_OK;
 }
 

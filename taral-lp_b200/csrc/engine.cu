@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdlib>
@@ -34,6 +35,13 @@ namespace taral {
 // Device buffers come from the device's default memory pool (cudaMallocAsync / cudaFreeAsync on the context's
 // stream). The pool keeps up to 32 GB of freed memory for the process, so a context's release is a stream-ordered
 // return to the pool and the next context of the process reuses the memory without new device allocations.
+// Fault-injection hook (taral_set_device_alloc_limit): the most bytes one context or batch may allocate, 0 = no limit.
+static std::atomic<size_t> g_alloc_limit{0};
+bool alloc_allowed(size_t used, size_t more) {
+    const size_t lim = g_alloc_limit.load(std::memory_order_relaxed);
+    return lim == 0 || used + more <= lim;
+}
+
 void keep_pool_memory(int dev) {
     static std::mutex mu;
     static std::vector<int> done;
@@ -147,6 +155,8 @@ struct Engine final : EngineBase {
     U* alloc(size_t count) {  // stream-ordered, from the device's memory pool (see keep_pool_memory)
         void* p = nullptr;
         const size_t bytes = std::max<size_t>(count, 1) * sizeof(U);
+        if (!alloc_allowed(alloc_bytes, bytes))
+            throw CudaError{"cudaMalloc: the device allocation limit (taral_set_device_alloc_limit) is reached"};
         cudaError_t e = cudaMallocAsync(&p, bytes, st);
         if (e != cudaSuccess) throw CudaError{std::string("cudaMalloc: ") + cudaGetErrorString(e)};
         allocs.push_back(p);
@@ -193,6 +203,7 @@ struct Engine final : EngineBase {
         CK(cudaGetDeviceProperties(&prop, dev));
         name = prop.name;
         CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        if (const char* e = std::getenv("TARAL_PDL")) pdl = std::atoi(e) != 0;
     }
     void init(const taral_csr& hA, const taral_csr& hAT, const double* hc_ptr, const double* hl, const double* hu,
               const double* hrl_ptr, const double* hru_ptr, const double* hDr, const double* hDc, int m_, int n_,
@@ -471,15 +482,28 @@ struct Engine final : EngineBase {
     }
 
     // ------------------------------------------------------------------ SpMV-shaped launches
+    // `programmatic`: launch with programmatic stream serialisation, so the kernel may start while its predecessor
+    // drains (both phase kernels release their successor at entry and wait for their predecessor before the first
+    // gather). Used for the two phase kernels of an iteration block when TARAL_PDL is not 0.
+    template <class K, class... Args>
+    void launch(K kernel, int grid, bool programmatic, Args... args) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(unsigned(grid)), cfg.blockDim = dim3(kThreads), cfg.dynamicSmemBytes = 0, cfg.stream = st;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = attr, cfg.numAttrs = programmatic ? 1 : 0;
+        CK(cudaLaunchKernelEx(&cfg, kernel, args...));
+    }
     template <class X, class E>
-    void rowblock(const DevMat& a, const X* xin, const E& epi, const int* skip = nullptr) {
+    void rowblock(const DevMat& a, const X* xin, const E& epi, const int* skip = nullptr, bool programmatic = false) {
         if (a.nblk == 0) return;
         if (a.per_thread)
-            k_rowthread<T, X, E><<<(a.rows + kThreads - 1) / kThreads, kThreads, 0, st>>>(
-                a.rows, a.ptr, a.idx, static_cast<const T*>(a.val), xin, skip, epi);
+            launch(k_rowthread<T, X, E>, (a.rows + kThreads - 1) / kThreads, programmatic, a.rows,
+                   (const int*)a.ptr, (const int*)a.idx, static_cast<const T*>(a.val), xin, skip, epi);
         else
-            k_rowblock<T, X, E, true><<<a.nblk, kThreads, 0, st>>>(a.ptr, a.idx, static_cast<const T*>(a.val), xin,
-                                                                    a.blk, skip, epi);
+            launch(k_rowblock<T, X, E, true>, a.nblk, programmatic, (const int*)a.ptr, (const int*)a.idx,
+                   static_cast<const T*>(a.val), xin, (const int4*)a.blk, skip, epi);
         ++launches;
     }
     template <class X, class Y>
@@ -552,11 +576,12 @@ struct Engine final : EngineBase {
         CK(cudaGetLastError());
         started = true;
     }
+    bool pdl = true;  // TARAL_PDL=0: plain launches of the phase kernels (set at init)
     void launch_block(int steps) {
         k_xupd<T><<<grid_for(n), 256, 0, st>>>(n, x, ATz, c, l, u, par, xs);
         for (int s = 0; s < steps; ++s) {
-            rowblock(A, x, EpiRow<T>{Ax, z, zs, rl, ru, par});
-            rowblock(AT, z, EpiCol<T>{ATz, x, xs, c, l, u, par, s + 1 < steps ? 1 : 0});
+            rowblock(A, x, EpiRow<T>{Ax, z, zs, rl, ru, par}, nullptr, pdl);
+            rowblock(AT, z, EpiCol<T>{ATz, x, xs, c, l, u, par, s + 1 < steps ? 1 : 0}, nullptr, pdl);
         }
     }
     void iterate(int steps) override {
@@ -653,6 +678,43 @@ struct Engine final : EngineBase {
         float ms = 0;
         CK(cudaEventElapsedTime(&ms, ev0, ev1));
         return ms;
+    }
+    void scaled_values(double* hDr, double* hDc, double* a_val, double* at_val) override {
+        auto fetch = [&](const void* d, size_t k) {
+            std::vector<T> h(k);
+            if (k) CK(cudaMemcpyAsync(h.data(), d, k * sizeof(T), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            return std::vector<double>(h.begin(), h.end());
+        };
+        if (hDr) {
+            std::vector<double> v = fetch(Dr, size_t(m));
+            if (!rperm.empty()) v = to_model(v);
+            std::copy(v.begin(), v.end(), hDr);
+        }
+        if (hDc) {
+            const std::vector<double> v = fetch(Dc, size_t(n));
+            std::copy(v.begin(), v.end(), hDc);
+        }
+        if (at_val) {
+            const std::vector<double> v = fetch(AT.val, size_t(AT.nnz));
+            std::copy(v.begin(), v.end(), at_val);
+        }
+        if (a_val) {
+            const std::vector<double> v = fetch(A.val, size_t(A.nnz));
+            if (rperm.empty()) {
+                std::copy(v.begin(), v.end(), a_val);
+            } else {  // internal row k is model row rperm[k]: place each row at its model position
+                std::vector<int> ip(size_t(m) + 1);
+                if (m) CK(cudaMemcpyAsync(ip.data(), A.ptr, ip.size() * sizeof(int), cudaMemcpyDeviceToHost, st));
+                CK(cudaStreamSynchronize(st));
+                std::vector<int64_t> mp(size_t(m) + 1, 0);  // model-order row pointers
+                for (int k = 0; k < m; ++k) mp[size_t(rperm[size_t(k)]) + 1] = ip[size_t(k) + 1] - ip[size_t(k)];
+                for (int r = 0; r < m; ++r) mp[size_t(r) + 1] += mp[size_t(r)];
+                for (int k = 0; k < m; ++k)
+                    std::copy(v.begin() + ip[size_t(k)], v.begin() + ip[size_t(k) + 1],
+                              a_val + mp[size_t(rperm[size_t(k)])]);
+            }
+        }
     }
     void profile_phases(int reps, double* row_ms, double* col_ms) override {
         // reps row-phase launches back to back, then reps column-phase launches, each run bracketed by events:
@@ -867,9 +929,14 @@ extern "C" int pdhg_info(pdhg_ctx* ctx, char* name_out, size_t cap, size_t* mem_
     if (mem_used) *mem_used = ctx->e->mem_used;
     return TARAL_OK;
 }
+extern "C" int pdhg_scaled_problem(pdhg_ctx* ctx, double* Dr, double* Dc, double* A_val, double* AT_val) {
+    if (!ctx) return TARAL_ERR_INPUT;
+    GUARD(ctx, ctx->e->scaled_values(Dr, Dc, A_val, AT_val))
+}
 extern "C" int64_t pdhg_kernel_launches(const pdhg_ctx* ctx) { return ctx ? ctx->e->launches : 0; }
 extern "C" const char* pdhg_last_error(const pdhg_ctx* ctx) { return ctx ? ctx->err.c_str() : "NULL context"; }
 extern "C" void pdhg_destroy(pdhg_ctx* ctx) { delete ctx; }
+extern "C" void taral_set_device_alloc_limit(size_t bytes) { taral::g_alloc_limit.store(bytes); }
 
 // ================================================================================================ SpMV plan
 struct taral_spmv_plan {

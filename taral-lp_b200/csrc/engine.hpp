@@ -35,6 +35,10 @@ struct EngineBase {
     // `reps` PDHG iterations launched one kernel at a time, each row-phase and column-phase kernel bracketed by
     // CUDA events on the context stream; average milliseconds per launch of each.
     virtual void profile_phases(int reps, double* row_ms, double* col_ms) = 0;
+    // The scaling factors and scaled matrix values held on the device, widened to double, in the model's row order
+    // (any pointer may be NULL): Dr (m), Dc (n), A's values (nnz, rows in the model's order, each row's entries in
+    // column order), A^T's values (nnz, A^T's entry order).
+    virtual void scaled_values(double* Dr, double* Dc, double* a_val, double* at_val) = 0;
     // Host copies of the scaled c, rl, ru kept at creation (the driver's step-size and norm set-up reads them).
     std::vector<double> hc, hrl, hru;
 };
@@ -45,6 +49,8 @@ void engine_init(EngineBase& e, int precision, const taral_csr& A, const taral_c
                  const double* Dc, int m, int n, int eval_freq, unsigned flags);
 std::vector<int4> build_row_blocks(const int64_t* ptr, int rows);
 void keep_pool_memory(int dev);  // the device pool keeps freed memory for reuse by later contexts
+// False when `more` bytes on top of `used` would pass the limit set by taral_set_device_alloc_limit.
+bool alloc_allowed(size_t used, size_t more);
 // Blocks of at most `tile` nonzeros and `rows_max` rows (a longer row is a block of its own).
 std::vector<int4> build_row_blocks(const int64_t* ptr, int rows, int tile, int rows_max);
 // The block list with the flags of row-split policy 0..4 (kernels.cuh, kPolicies); returns false when the policy

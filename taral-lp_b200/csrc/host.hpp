@@ -122,7 +122,7 @@ Outcome run(B& b, const DriverData& P, const Options& o, double time_budget, con
         sch.iterations += block, sch.since_restart += block;
         const double f = 1.0 / double(sch.since_restart);
         b.eval_pair(f, cur, avg);
-        last = judge_block(sch, cur, avg, rule, since(t0) > time_budget);
+        last = judge_block(sch, cur, avg, rule, since(t0) > time_budget ? int(TARAL_TIME_LIMIT) : -1);
         if (o.verbose && (sch.iterations / o.eval_freq) % 50 == 0)
             std::fprintf(stderr, "[pdhg] iter=%lld weight=%.3e best(p,d,gap)=(%.2e, %.2e, %.2e) from=%s c'x=%.10g\n",
                          (long long)sch.iterations, sch.weight, last.best.primal, last.best.dual, last.best.gap,

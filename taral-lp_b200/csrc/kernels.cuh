@@ -59,6 +59,13 @@ __device__ __forceinline__ double gather(const double* p) {
     return v;
 }
 
+// Programmatic dependent launch (sm_90+): a phase kernel lets its successor in the stream start as soon as every one
+// of its own CTAs is running (pdl_release), and waits for its predecessor grid to complete, with its memory visible,
+// before touching anything the predecessor writes (pdl_acquire). Without the launch attribute (a plain launch, or
+// the first kernel after a non-programmatic one) the wait returns at once, so every kernel may call both.
+__device__ __forceinline__ void pdl_release() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_acquire() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // Products rounded on their own (never fused into a following add), as the staged paths round them.
 __device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
@@ -256,6 +263,7 @@ __device__ __forceinline__ void block_sums(const int* __restrict__ ptr, const in
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int r0 = meta.x, nrows = meta.y & 0xffff, p0 = meta.z, p1 = meta.w, len = p1 - p0;
     if (len > kTile) {  // one long row: strided partial sums, fixed-order block reduction
+        pdl_acquire();
         double s = 0;
         if (VEC) {
             const int a0 = p0 & ~3;
@@ -310,6 +318,7 @@ __device__ __forceinline__ void block_sums(const int* __restrict__ ptr, const in
                 }
             }
         }
+        pdl_acquire();  // the matrix stream above is constant; the gathered vector is the predecessor's output
         X g[kQuads][4];
 #pragma unroll
         for (int i = 0; i < kQuads; ++i)
@@ -336,6 +345,7 @@ __device__ __forceinline__ void block_sums(const int* __restrict__ ptr, const in
             }
         }
     } else {
+        pdl_acquire();
         for (int k = p0 + tid; k < p1; k += kThreads)
             sm.prod[seg ? k - base : pidx(k - p0)] = P(__ldg(val + k)) * P(__ldg(xin + __ldg(idx + k)));
     }
@@ -402,13 +412,17 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_rowblock(const int* __
                                                          E epi) {
     using P = typename ProdT<T, X>::type;
     __shared__ RowSmem<P> sm;
-    if (skip && *skip) return;
+    pdl_release();
+    if (skip) {  // a flag the predecessor may set
+        pdl_acquire();
+        if (*skip) return;
+    }
     const int tid = threadIdx.x;
     const int4 meta = __ldg(blk + blockIdx.x);
     const int r0 = meta.x, nrows = meta.y & 0xffff;
     typename E::Ops ops{};
     const bool mine = tid < nrows;
-    if (mine) ops = epi.load(r0 + tid, 0);
+    if (mine) ops = epi.load(r0 + tid, 0);  // this phase's own vectors: the other phase does not write them
     block_sums<T, X, VEC>(ptr, idx, val, xin, meta, sm);
     if (mine) epi.apply(r0 + tid, sm.rowsum[tid], ops);
 }
@@ -423,11 +437,16 @@ __global__ void __launch_bounds__(kThreads) k_rowthread(int rows, const int* __r
                                                         const X* __restrict__ xin, const int* __restrict__ skip,
                                                         E epi) {
     using P = typename ProdT<T, X>::type;
-    if (skip && *skip) return;
+    pdl_release();
+    if (skip) {
+        pdl_acquire();
+        if (*skip) return;
+    }
     const int r = blockIdx.x * kThreads + threadIdx.x;
     if (r >= rows) return;
     const typename E::Ops ops = epi.load(r, 0);
     const int a = __ldg(ptr + r), b = __ldg(ptr + r + 1);
+    pdl_acquire();
     double s = 0;
     for (int k = a; k < b; ++k) s += double(mul_rn(P(__ldg(val + k)), P(gather(xin + __ldg(idx + k)))));
     epi.apply(r, s, ops);

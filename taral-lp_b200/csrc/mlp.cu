@@ -6,12 +6,14 @@
 // Forward per layer: C = H_{l-1} W_l (GEMM, FP32 accumulate), Z = C + b, H = bf16(gelu(Z)) (last layer: Y = Z).
 // Backward: dW = H_{l-1}^T dZ, db = sum_b dZ, dH_{l-1} = dZ W_l^T, dZ = dH * gelu'(Z); loss = mean (Y - T)^2.
 //
-// GEMMs: the forward pass runs on the tcgen05 tensor cores (mlp_tc.cu: C = H Wt^T with Wt = W^T kept as a bf16
-// [out][in] copy, refreshed whenever the weights change) for every layer whose input width is a multiple of 8.
-// The backward pass (and any other layer) uses mma.sync m16n8k16 (bf16 x bf16 -> f32), 128 x 128 x 32 CTA tiles,
-// 8 warps of 64 x 32, operands staged in shared memory and fed with ldmatrix; A may be stored transposed (TA: A =
-// X^T) and B as [N][K] (TB: B = W^T); split-K writes per-slice partials that a second kernel adds in slice order
-// (deterministic).
+// GEMMs: for every layer whose input width is a multiple of 8 (and whose dZ rows are 16-byte multiples: the output
+// gradient of the last layer is stored with its row stride rounded up to 8) all three GEMMs run on the tcgen05 tensor
+// cores through TMA (mlp_tc.cu, gemm_umma): the forward C = H Wt^T with Wt = W^T kept as a bf16 [out][in] copy
+// refreshed whenever the weights change (both operands K-major), dW = H_prev^T dZ (both operands read MN-major) and
+// dH_prev = dZ W^T (dZ K-major, Wt MN-major, K split into slices summed in order). Any other layer uses mma.sync
+// m16n8k16 (bf16 x bf16 -> f32), 128 x 128 x 32 CTA tiles, 8 warps of 64 x 32, operands staged in shared memory and
+// fed with ldmatrix; A may be stored transposed (TA: A = X^T) and B as [N][K] (TB: B = W^T); split-K writes per-slice
+// partials that a second kernel adds in slice order (deterministic).
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -28,6 +30,8 @@
 namespace taral {
 namespace tc {
 int gemm_tc(int M, int N, int K, const void* A, const void* Bt, float* C, int* err, cudaStream_t stream);
+int gemm_umma(int M, int N, int K, const void* A, int lda, int a_mn, const void* B, int ldb, int b_mn, float* C,
+              int ldc, int slices, float* ws, int* err, cudaStream_t stream);
 }
 namespace mlp {
 
@@ -188,7 +192,7 @@ __global__ void k_bias_act(int rows, int cols, const float* __restrict__ C, cons
 }
 
 // R = Y - T (FP32), dY = bf16(2 R / (rows * cols)); per-row partial sums of R^2 into part[row].
-__global__ void k_loss_grad(int rows, int cols, const float* __restrict__ Y, const float* __restrict__ T,
+__global__ void k_loss_grad(int rows, int cols, int ldy, const float* __restrict__ Y, const float* __restrict__ T,
                             float* __restrict__ R, bf16* __restrict__ dY, double* __restrict__ part) {
     const int row = blockIdx.x;
     const float scale = 2.f / (float(rows) * float(cols));
@@ -197,7 +201,7 @@ __global__ void k_loss_grad(int rows, int cols, const float* __restrict__ Y, con
         const size_t i = size_t(row) * cols + j;
         const float r = Y[i] - T[i];
         R[i] = r * scale;
-        dY[i] = __float2bfloat16(r * scale);
+        dY[size_t(row) * ldy + j] = __float2bfloat16(r * scale);  // row stride ldy >= cols (padded for TMA)
         s += double(r) * double(r);
     }
     for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
@@ -294,6 +298,7 @@ struct Mlp {
     bf16* Xb = nullptr;  // input batch
     float *Xf = nullptr, *Tf = nullptr, *C = nullptr, *R = nullptr, *dHf = nullptr, *dZf = nullptr, *ws = nullptr;
     bf16 *dYb = nullptr, *dZb = nullptr;
+    int ldy = 0;  // row stride of dYb: the output width, rounded up to 8 when the last layer's backward runs on tcgen05
     double* part = nullptr;
     int* d_idx = nullptr;
     int* d_err = nullptr;  // set by the tcgen05 GEMM when a completion wait gave up
@@ -341,7 +346,8 @@ struct Mlp {
         }
         size_t widest = std::max<size_t>(size_t(out), size_t(hid));
         Xb = alloc<bf16>(size_t(mb) * in), Xf = alloc<float>(size_t(mb) * in), Tf = alloc<float>(size_t(mb) * out);
-        C = alloc<float>(size_t(mb) * widest), R = alloc<float>(size_t(mb) * out), dYb = alloc<bf16>(size_t(mb) * out);
+        ldy = L[depth].Wt ? (out + 7) / 8 * 8 : out;
+        C = alloc<float>(size_t(mb) * widest), R = alloc<float>(size_t(mb) * out), dYb = alloc<bf16>(size_t(mb) * ldy);
         dHf = alloc<float>(size_t(mb) * widest), dZf = alloc<float>(size_t(mb) * hid), dZb = alloc<bf16>(size_t(mb) * hid);
         part = alloc<double>(mb), d_idx = alloc<int>(mb), d_err = alloc<int>(1);
         MK(cudaMemsetAsync(d_err, 0, sizeof(int), s));
@@ -411,20 +417,40 @@ struct Mlp {
 
     double backward(int batch) {  // needs forward(batch) and Tf; fills gW, gb; returns the loss
         Layer& top = L[depth];
-        k_loss_grad<<<batch, 256, 0, s>>>(batch, top.out, top.Z, Tf, R, dYb, part);
+        k_loss_grad<<<batch, 256, 0, s>>>(batch, top.out, ldy, top.Z, Tf, R, dYb, part);
         const bf16* dZ = dYb;
         const float* dZfl = R;
+        int ldz = ldy;  // row stride of dZ
         for (int l = depth; l >= 0; --l) {
             Layer& y = L[l];
             const bf16* Hprev = l > 0 ? L[l - 1].H : Xb;
-            gemm<true, false>(y.in, y.out, batch, Hprev, dZ, y.gW);              // dW = H_prev^T dZ
+            // tcgen05 when the operands fit TMA (16-byte rows): dW = H_prev^T dZ reads both operands MN-major,
+            // dH_prev = dZ W^T reads dZ K-major and W^T (kept as Wt [out][in]) MN-major; mma.sync otherwise
+            const bool tc = y.Wt && ldz % 8 == 0;
+            if (tc) {
+                if (taral::tc::gemm_umma(y.in, y.out, batch, Hprev, y.in, 1, dZ, ldz, 1, y.gW, y.out, 1, nullptr, d_err, s) !=
+                    TARAL_OK)
+                    throw MlpError{std::string("tcgen05 GEMM launch: ") + cudaGetErrorString(cudaGetLastError())};
+            } else {
+                gemm<true, false>(y.in, y.out, batch, Hprev, dZ, y.gW);              // dW = H_prev^T dZ
+            }
             k_colsum<<<grid1(y.out), 256, 0, s>>>(batch, y.out, dZfl, y.gb);     // db = sum_b dZ
             if (l > 0) {
-                int slices = std::max(1, std::min(64, y.out / 2048));
-                gemm<false, true>(batch, y.in, y.out, dZ, y.Wb, dHf, slices);    // dH_prev = dZ W^T
+                if (tc) {
+                    const int tiles = ((batch + 127) / 128) * ((y.in + 255) / 256);
+                    const size_t per_slice = size_t(batch) * y.in;
+                    const int slices = int(std::max<size_t>(1, std::min<size_t>(std::max(1, 148 / tiles),
+                                                                                ws_count / per_slice)));
+                    if (taral::tc::gemm_umma(batch, y.in, y.out, dZ, ldz, 0, y.Wt, y.in, 1, dHf, y.in, slices, ws, d_err, s) !=
+                        TARAL_OK)
+                        throw MlpError{std::string("tcgen05 GEMM launch: ") + cudaGetErrorString(cudaGetLastError())};
+                } else {
+                    int slices = std::max(1, std::min(64, y.out / 2048));
+                    gemm<false, true>(batch, y.in, y.out, dZ, y.Wb, dHf, slices);    // dH_prev = dZ W^T
+                }
                 Layer& p = L[l - 1];
                 k_gelu_back<<<grid1(size_t(batch) * p.out), 256, 0, s>>>(size_t(batch) * p.out, dHf, p.Z, dZf, dZb);
-                dZ = dZb, dZfl = dZf;
+                dZ = dZb, dZfl = dZf, ldz = p.out;
             }
         }
         std::vector<double> h(batch);

@@ -137,14 +137,15 @@ struct BlockDecision {
 
 // Judge one block from the evaluations of the current point `cur` and of the average `avg` (the schedule's
 // iteration counters already include the block). Stops on a non-finite error at both points
-// (numerical_failure), on the better point's worst relative error <= tol (near_optimal), on `out_of_time`
-// (time_limit) or on the iteration cap (iteration_limit), in that order. Otherwise the candidate (the point with
+// (numerical_failure), on the better point's worst relative error <= tol (near_optimal), on an external stop
+// request `stop` (a taral_solve_status such as time_limit or cancelled; -1: none) or on the iteration cap
+// (iteration_limit), in that order. Otherwise the candidate (the point with
 // the lower weighted error) restarts when a long time has passed since the last restart (36 % of all iterations),
 // when its error fell to 20 % of the anchor, or when it fell to 80 % and rose since the last block; a restart
 // re-anchors the schedule and, when both movements ||dx||, ||dz|| exceed 1e-10, moves log w halfway to
 // log(||dz|| / ||dx||).
 TARAL_HD BlockDecision judge_block(Schedule& s, const double* cur, const double* avg, const StopRule& rule,
-                                   bool out_of_time) {
+                                   int stop) {
     BlockDecision d;
     const Residuals rc = residuals_of(cur, rule), ra = residuals_of(avg, rule);
     const double ec = rc.worst(), ea = ra.worst();
@@ -153,7 +154,7 @@ TARAL_HD BlockDecision judge_block(Schedule& s, const double* cur, const double*
     d.status = -1, d.restart = kNoRestart, d.new_weight = false;
     if (!sched::finite(ec) && !sched::finite(ea)) d.status = TARAL_NUMERICAL_FAILURE;
     else if (d.best.worst() <= rule.tol) d.status = TARAL_NEAR_OPTIMAL;
-    else if (out_of_time) d.status = TARAL_TIME_LIMIT;
+    else if (stop >= 0) d.status = stop;
     else if (s.iterations >= rule.max_iter) d.status = TARAL_ITERATION_LIMIT;
     if (d.status >= 0) return d;
 

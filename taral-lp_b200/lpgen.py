@@ -156,9 +156,42 @@ class LP:
             f.write(self.mps_text())
 
 
-def _r12(v):
+def _r12_text(v):
     """Round doubles through the '%.12g' text the MPS writer emits (what a reader of that file sees)."""
     return np.char.mod("%.12g", np.asarray(v, np.float64)).astype(np.float64)
+
+
+_POW10 = np.array([10.0 ** k for k in range(23)])  # exactly representable powers of ten
+
+
+def _r12(v):
+    """The same doubles as _r12_text, computed arithmetically: with e the decimal exponent of |v| and k = 11 - e,
+    M = the integer nearest to v * 10^k (12 significant digits) and the result M / 10^k (or M * 10^-k), one
+    correctly rounded IEEE operation on two exact operands, i.e. the double nearest to the decimal M * 10^-k, which
+    is what reading the 12-digit text gives. Values where the float product v * 10^k lies within 4 ulps of a
+    rounding tie, near a power of ten, or outside 10^-11 .. 10^22 go through the text instead."""
+    v0 = np.asarray(v, np.float64)
+    v = v0.ravel()
+    out = v.copy()
+    idx = np.nonzero(np.isfinite(v) & (v != 0))[0]
+    if idx.size == 0:
+        return out.reshape(v0.shape)
+    a = np.abs(v[idx])
+    lg = np.log10(a)
+    e = np.floor(lg).astype(np.int64)
+    k = 11 - e
+    ok = (np.abs(lg - np.rint(lg)) > 1e-9) & (k >= 0) & (k <= 22)
+    kk = np.clip(k, 0, 22)
+    scaled = a * _POW10[kk]
+    M = np.rint(scaled)
+    tie = np.abs(scaled - np.floor(scaled) - 0.5) <= 4 * np.spacing(scaled)
+    ok &= ~tie & (M >= 1e11) & (M <= 1e12)
+    r = np.copysign(M / _POW10[kk], v[idx])
+    out[idx[ok]] = r[ok]
+    rest = idx[~ok]
+    if rest.size:
+        out[rest] = _r12_text(v[rest])
+    return out.reshape(v0.shape)
 
 
 def _csc_from_lists(n, rows_per_col, vals_per_col, keep=None):

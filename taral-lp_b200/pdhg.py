@@ -21,12 +21,13 @@ LIB_PATH = PKG / "lib" / "libtaral_pdhg.so"
 CLI_PATH = PKG / "bin" / "pdhg"
 
 OK, ERR_CUDA, ERR_ALLOC, ERR_INPUT, ERR_UNSUPPORTED, ERR_PARSE, ERR_STATE, ERR_NO_DEVICE = 0, -1, -2, -3, -4, -5, -6, -7
+ERR_CANCELLED = -8
 FP64, FP32 = 0, 1
-STATUS = {0: "near_optimal", 1: "iteration_limit", 2: "time_limit", 3: "numerical_failure"}
+STATUS = {0: "near_optimal", 1: "iteration_limit", 2: "time_limit", 3: "numerical_failure", 4: "cancelled"}
 KKT_NAMES = ["PR2S", "PR2O", "PR2R", "DROW", "DZ2", "DR2S", "DR2O", "POBJ", "DCOL", "DX2"]
 ERRORS = {ERR_CUDA: "CUDA error", ERR_ALLOC: "allocation failed", ERR_INPUT: "bad input",
           ERR_UNSUPPORTED: "unsupported model", ERR_PARSE: "parse error", ERR_STATE: "call out of order",
-          ERR_NO_DEVICE: "no CUDA device"}
+          ERR_NO_DEVICE: "no CUDA device", ERR_CANCELLED: "cancelled"}
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)
@@ -109,6 +110,9 @@ SIGNATURES = {
                                    C.POINTER(C.c_int64)]),
     "taral_batch_last_error": (C.c_char_p, [C.c_void_p]),
     "taral_batch_destroy": (None, [C.c_void_p]),
+    "taral_batch_cancel": (C.c_int, [C.c_void_p]),
+    "pdhg_scaled_problem": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp]),
+    "taral_set_device_alloc_limit": (None, [C.c_size_t]),
     "taral_check_models": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "taral_kkt_eval_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double] + [C.c_void_p] * 13 +
                                [C.c_void_p, C.c_void_p]),
@@ -127,6 +131,9 @@ SIGNATURES = {
                                   C.c_int, C.c_void_p, C.c_void_p]),
     "taral_gemm_bf16_tc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                      C.c_void_p]),
+    "taral_gemm_bf16_umma": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_void_p,
+                                       C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                                       C.c_void_p]),
     "taral_spmv_plan_create": (C.c_int, [C.c_int, C.c_int, _lp, C.c_int, C.POINTER(C.c_void_p)]),
     "taral_spmv_run": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                  C.c_void_p]),
@@ -272,6 +279,13 @@ class Engine:
         out["status"] = STATUS[r.status]
         return out, (None if x is None else x[:self.n]), (None if z is None else z[:self.m])
 
+    def scaled_problem(self, nnz):
+        """(Dr, Dc, A values, A^T values) of the scaled problem held on the device (pdhg_scaled_problem)."""
+        dr, dc = np.zeros(max(self.m, 1)), np.zeros(max(self.n, 1))
+        a, at = np.zeros(max(nnz, 1)), np.zeros(max(nnz, 1))
+        _check(lib().pdhg_scaled_problem(self.h, _p(dr), _p(dc), _p(a), _p(at)), self.h)
+        return dr[:self.m], dc[:self.n], a[:nnz], at[:nnz]
+
     def profile_phases(self, reps):
         """Mean CUDA-event milliseconds per launch of the row-phase and column-phase kernels over `reps` steps."""
         a, b = C.c_double(), C.c_double()
@@ -332,6 +346,12 @@ def solve(lp, tol=1e-4, time_limit=3600.0, max_iter=2_000_000_000, eval_freq=64,
     out = {k: getattr(r, k) for k, _ in OutcomeT._fields_}
     out["status"] = STATUS[r.status]
     return out, x[:lp.n], y[:lp.m]
+
+
+def set_device_alloc_limit(nbytes):
+    """Fault-injection hook for tests (taral_set_device_alloc_limit): contexts and batches created from now on fail
+    with ERR_ALLOC when their device allocations would exceed `nbytes`; 0 removes the limit."""
+    lib().taral_set_device_alloc_limit(int(nbytes))
 
 
 # ------------------------------------------------------------------------------------------------ check
@@ -417,7 +437,8 @@ class Batch:
             raise ValueError("w0 needs one entry per instance")
         code = lib().taral_batch_solve(self.h, tabs[0][1], tabs[1][1], None if wv is None else wv.ctypes.data,
                                        C.cast(outs, C.c_void_p), tabs[2][1], tabs[3][1])
-        if code != OK:
+        self.last_code = code  # ERR_CANCELLED: stopped by cancel(); the outcomes and points are filled all the same
+        if code not in (OK, ERR_CANCELLED):
             raise TaralError(code, (lib().taral_batch_last_error(self.h) or b"").decode())
         res = []
         for i in range(k):
@@ -427,6 +448,10 @@ class Batch:
         if not want_points:
             return res, None, None
         return res, [xout[i][:self.lps[i].n] for i in range(k)], [yout[i][:self.lps[i].m] for i in range(k)]
+
+    def cancel(self):
+        """Ask a running solve() (in another thread) to stop after its current block; see taral_batch_cancel."""
+        _check(lib().taral_batch_cancel(self.h))
 
     def close(self):
         if getattr(self, "h", None):

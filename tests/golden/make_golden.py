@@ -14,11 +14,15 @@ Needs the reference checkout (REF, default: the directory "reference" beside thi
                          (gpu/vector_check.check_files) on the .sol / .dual of the runs in reference_runs.json
 * reference_refinery_T4.json (with --refinery, ~2 minutes of CPU) the reference dual simplex optimum of one
                          4-period scenario of the refinery family (RefineryBase(48, seed=7), perturbations(2, seed=3)[0])
+* reference_ledger.json  (with --ledger) the reference harness's ledger contract, read from gpu/bench_pdhg.py: its
+                         FIELDS, the keys it reads from a PDHG JSON report, the flags it passes to the PDHG binary,
+                         and the row it writes for packing_10000 at 1e-6 when it runs the reference binary
+                         (--configs cpu1, the reference objective given through --ref-json)
 * reference_bench_lp.json (with --bench-lp, minutes of CPU) the reference `pdhg --device cpu` FP64 report on the
                          benchmark LP (planted, Zipf rows, 200,000 x 500,000, seed 0) solved to 1e-6: the FP64
                          iteration count the benchmark's CPU baselines are projected to
 
-Run from the repository root: python tests/golden/make_golden.py [--bench-lp | --refinery | --vector-check]
+Run from the repository root: python tests/golden/make_golden.py [--bench-lp | --refinery | --vector-check | --ledger]
 """
 import csv
 import hashlib
@@ -178,8 +182,42 @@ def refinery():
     print("wrote reference_refinery_T4.json:", out["status"], out["objective"])
 
 
+def ledger():
+    import ast
+    import re
+    harness = REF / "gpu" / "bench_pdhg.py"
+    src = harness.read_text()
+    tree = ast.parse(src)
+    fields = next(ast.literal_eval(n.value) for n in ast.walk(tree)
+                  if isinstance(n, ast.Assign) and any(getattr(t, "id", None) == "FIELDS" for t in n.targets))
+    json_keys = sorted(set(re.findall(r"r0\.get\('([a-z_0-9]+)'\)", src)) | set(re.findall(r"med\('([a-z_0-9]+)'\)", src)))
+    run_pdhg = next(n for n in ast.walk(tree) if isinstance(n, ast.FunctionDef) and n.name == "run_pdhg")
+    flags = sorted({c.value for c in ast.walk(run_pdhg) if isinstance(c, ast.Constant) and isinstance(c.value, str)
+                    and c.value.startswith("--")})
+    pins = json.loads((OUT / "ledger_pins.json").read_text())["packing_10000_tol1e-6"]
+    lp = lpgen.packing(10000, seed=1)
+    with tempfile.TemporaryDirectory() as td:
+        td = Path(td)
+        f = td / "packing_10000.mps"
+        lp.write_mps(f)
+        refs = td / "refs.json"
+        refs.write_text(json.dumps({"packing_10000": float(pins["objective"])}))
+        env = dict(os.environ, TARAL_PDHG=str(PDHG))
+        subprocess.run([sys.executable, str(harness), str(f), "--out", str(td / "led"), "--configs", "cpu1",
+                        "--tol", "1e-6", "--repeats", "1", "--ref-json", str(refs)], check=True, env=env,
+                       stdout=subprocess.DEVNULL)
+        row = json.loads((td / "led.json").read_text())["rows"][0]
+    out = {"harness": "gpu/bench_pdhg.py", "fields": fields, "json_keys": json_keys, "pdhg_flags": flags,
+           "model_sha256": lp.digest(), "reference_objective_via_ref_json": float(pins["objective"]),
+           "reference_row_cpu1": row}
+    (OUT / "reference_ledger.json").write_text(json.dumps(out, indent=1) + "\n")
+    print("wrote reference_ledger.json:", len(fields), "fields,", row["status"], row["iterations"])
+
+
 if __name__ == "__main__":
-    if "--bench-lp" in sys.argv:
+    if "--ledger" in sys.argv:
+        ledger()
+    elif "--bench-lp" in sys.argv:
         bench_lp()
     elif "--refinery" in sys.argv:
         refinery()

@@ -55,3 +55,18 @@ def test_general_planted_points_feasible():
     kinds = {(np.isfinite(a), np.isfinite(b)) for a, b in zip(lp.col_lo, lp.col_up)}
     assert kinds == {(False, False), (True, False), (False, True), (True, True)}
     assert np.any(lp.col_lo == lp.col_up) and np.any(np.isfinite(lp.row_lo) & np.isfinite(lp.row_up) & (lp.row_lo < lp.row_up))
+
+
+def test_r12_arithmetic_equals_text_rounding():
+    """The arithmetic 12-digit rounding used by the generators gives the doubles of the '%.12g' text, bit for bit,
+    on wide-range values, the generators' price and capacity products, ties, powers of ten and specials."""
+    rng = np.random.default_rng(11)
+    cases = [rng.standard_normal(200_000) * np.exp(rng.uniform(-25, 25, 200_000)),
+             np.round(rng.uniform(-50, 50, 100_000), 4) * rng.uniform(0.8, 1.2, 100_000),
+             np.round(rng.uniform(100, 1000, 100_000), 3) * rng.uniform(0.8, 1.2, 100_000),
+             (rng.integers(1, 10**12, 50_000) * 2 + 1) / 2.0 / 10.0 ** rng.integers(0, 12, 50_000),
+             np.array([10.0 ** k for k in range(-30, 30)] + [-(10.0 ** k) for k in range(-30, 30)]),
+             np.array([0.0, -0.0, np.inf, -np.inf, np.nan, 5e-324, 1.7e308, 999999999999.5, 0.1, 1 / 3])]
+    for v in cases:
+        a, b = lpgen._r12(v), lpgen._r12_text(v)
+        assert np.array_equal(a, b, equal_nan=True) and np.array_equal(np.signbit(a), np.signbit(b))

@@ -196,3 +196,26 @@ def test_row_order_fp32(engine_lib, monkeypatch):
     xb, zb = eng.download(0, 1.0)
     assert np.array_equal(xb, xs.astype(np.float32).astype(np.float64))
     assert np.array_equal(zb, zs.astype(np.float32).astype(np.float64))
+
+
+@pytest.mark.parametrize("precision", [pdhg.FP64, pdhg.FP32], ids=["fp64", "fp32"])
+def test_device_scaling_equals_host_scaling(engine_lib, oracle_lib, precision):
+    """The set-up scales the model on the device (Ruiz x10, then Pock-Chambolle, in FP64 with the reference's
+    operation order): Dr, Dc and the scaled values of A and A^T equal the oracle's host restatement of
+    gpu/pdhg.cu:80-133 element by element (FP32 contexts: the same values narrowed to float). The models cover
+    explicit zeros in the columns, a maximisation, power-law rows (FP32: rows held in length order internally),
+    free and fixed columns."""
+    zeros = lpgen.general(250, 600, seed=8)
+    zeros.val = zeros.val.copy()
+    zeros.val[::17] = 0.0  # explicit zeros: dropped before scaling, as the reference's column-wise copy drops them
+    models = [zeros, lpgen.general(300, 700, seed=3, maximize=True), lpgen.packing(3000, seed=2),
+              lpgen.planted(3000, 8000, 6, seed=2, zipf=1.2, cap=400, floor=3), lpgen.transport(20, 30, seed=4)]
+    narrow = (lambda v: v) if precision == pdhg.FP64 else (lambda v: np.asarray(v).astype(np.float32).astype(np.float64))
+    for lp in models:
+        sp = oracle.ScaledProblem(lp)
+        eng = pdhg.Engine.from_model(lp, precision=precision)
+        dr, dc, a, at = eng.scaled_problem(len(sp.A[2]))
+        assert np.array_equal(dr, narrow(sp.Dr)) and np.array_equal(dc, narrow(sp.Dc)), lp.name
+        assert np.array_equal(a, narrow(sp.A[2])) and np.array_equal(at, narrow(sp.AT[2])), lp.name
+        assert eng.bnorm == sp.bnorm and eng.cnorm == sp.cnorm, lp.name
+        eng.close()

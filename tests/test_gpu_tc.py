@@ -51,3 +51,63 @@ def test_gemm_tc_rejects_bad_shapes(engine_lib):
                                          C.c_void_p(err.data_ptr()), None) == pdhg.ERR_INPUT  # K % 8
     assert pdhg.lib().taral_gemm_bf16_tc(4, 4, 8, C.c_void_p(d.data_ptr() + 2), p, C.c_void_p(out.data_ptr()),
                                          C.c_void_p(err.data_ptr()), None) == pdhg.ERR_INPUT  # misaligned A
+
+
+def _umma(M, N, K, a_mn, b_mn, lda_pad=0, ldb_pad=0, ldc_pad=0, slices=1, seed=0):
+    """taral_gemm_bf16_umma on operands stored in the given layouts (with padded row strides) against numpy."""
+    import torch
+    rng = np.random.default_rng(seed + 17 * M + 3 * N + K)
+    A = mlp_oracle.bf16(rng.standard_normal((M, K)))
+    B = mlp_oracle.bf16(rng.standard_normal((N, K)))
+    dev = torch.device("cuda")
+
+    def stored(X, mn, pad):  # X is (rows, K): K-major storage [rows][ld], MN-major storage [K][ld]
+        S = X.T if mn else X
+        ld = S.shape[1] + pad
+        buf = np.zeros((S.shape[0], ld))
+        buf[:, :S.shape[1]] = S
+        return torch.tensor(buf, dtype=torch.bfloat16, device=dev), ld
+    dA, lda = stored(A, a_mn, lda_pad)
+    dB, ldb = stored(B, b_mn, ldb_pad)
+    ldc = N + ldc_pad
+    dC = torch.full((M, ldc), float("nan"), dtype=torch.float32, device=dev)
+    ws = torch.zeros(max(slices, 1) * M * ldc, dtype=torch.float32, device=dev)
+    err = torch.zeros(1, dtype=torch.int32, device=dev)
+    code = pdhg.lib().taral_gemm_bf16_umma(M, N, K, C.c_void_p(dA.data_ptr()), lda, a_mn, C.c_void_p(dB.data_ptr()),
+                                           ldb, b_mn, C.c_void_p(dC.data_ptr()), ldc, slices,
+                                           C.c_void_p(ws.data_ptr()), C.c_void_p(err.data_ptr()), None)
+    assert code == pdhg.OK
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    got = dC.cpu().numpy().astype(np.float64)
+    ref = A @ B.T
+    assert np.all(np.isfinite(got[:, :N]))
+    if ldc_pad:
+        assert np.all(np.isnan(got[:, N:]))  # the padding of C is left alone
+    assert np.max(np.abs(got[:, :N] - ref)) <= 1e-5 * np.sqrt(K) * np.max(np.abs(ref)) + 1e-6, (M, N, K, a_mn, b_mn)
+
+
+@pytest.mark.parametrize("a_mn,b_mn", [(0, 0), (0, 1), (1, 0), (1, 1)])
+@pytest.mark.parametrize("M,N,K", [(128, 256, 64), (256, 512, 256), (200, 300, 136), (64, 1000, 512)])
+def test_gemm_umma_layouts(engine_lib, a_mn, b_mn, M, N, K):
+    _umma(M, N, K, a_mn, b_mn)
+
+
+def test_gemm_umma_padded_strides_and_split_k(engine_lib):
+    _umma(256, 1001, 256, 1, 1, lda_pad=0, ldb_pad=7, ldc_pad=5)          # dW-shaped: both MN-major, padded dZ
+    _umma(256, 512, 4096, 0, 1, lda_pad=8, ldb_pad=0, slices=9)           # dH-shaped: split K into slices
+    _umma(256, 33001, 512, 0, 0)                                          # forward-shaped, ragged N
+    _umma(100, 120, 1000, 1, 0, slices=64)                                # more slices than K blocks: clipped
+
+
+def test_gemm_umma_rejects_bad_strides(engine_lib):
+    import torch
+    d = torch.zeros(4096, dtype=torch.bfloat16, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    out = torch.zeros(4096, dtype=torch.float32, device="cuda")
+    p, o, e = C.c_void_p(d.data_ptr()), C.c_void_p(out.data_ptr()), C.c_void_p(err.data_ptr())
+    L = pdhg.lib()
+    assert L.taral_gemm_bf16_umma(8, 8, 16, p, 12, 0, p, 16, 0, o, 8, 1, None, e, None) == pdhg.ERR_INPUT  # lda % 8
+    assert L.taral_gemm_bf16_umma(8, 8, 16, p, 8, 0, p, 16, 0, o, 8, 1, None, e, None) == pdhg.ERR_INPUT   # lda < K
+    assert L.taral_gemm_bf16_umma(8, 8, 16, p, 16, 0, p, 16, 0, o, 4, 1, None, e, None) == pdhg.ERR_INPUT  # ldc < N
+    assert L.taral_gemm_bf16_umma(8, 8, 16, p, 16, 0, p, 16, 0, o, 8, 2, None, e, None) == pdhg.ERR_INPUT  # no ws
