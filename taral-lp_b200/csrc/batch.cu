@@ -560,6 +560,7 @@ struct Batch final : BatchBase {
         BK(cudaGetDevice(&dev));
         keep_pool_memory(dev);
         BK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        if (const char* e = std::getenv("TARAL_PDL")) pdl = std::atoi(e) != 0;
         // 1. distinct matrices (same sizes and identical col_ptr / row_idx / val)
         std::map<std::pair<uint64_t, std::pair<int, int>>, int> seen;
         std::map<std::tuple<const void*, const void*, const void*, int, int>, int> same_arrays;
@@ -930,16 +931,39 @@ struct Batch final : BatchBase {
     std::vector<int> first_inst;  // distinct matrix -> first instance that has it
 
     // ------------------------------------------------------------------ launches
+    // `programmatic`: the width-1 kernels of an iteration's two phases start while their predecessor drains (they
+    // release their successor at entry and wait for their predecessor before the first gather); TARAL_PDL=0 turns
+    // it off. The wide-pack kernel always launches plainly.
+    template <class K, class... Args>
+    void launch(K kernel, int grid, bool programmatic, Args... args) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(unsigned(grid)), cfg.blockDim = dim3(kThreads), cfg.dynamicSmemBytes = 0, cfg.stream = s;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = attr, cfg.numAttrs = programmatic ? 1 : 0;
+        BK(cudaLaunchKernelEx(&cfg, kernel, args...));
+        ++launches;
+    }
+    bool pdl = true;
     template <class X, class E>
-    void spmv_A(const X* xin, const E& e, const int* act) {
-        if (thread1[0] && nA1r) k_rowthread_batch<T, X, E><<<(nA1r + 7) / 8, kThreads, 0, s>>>(nA1r, Aptr, Aidx, Aval, xin, A1_rc, Ae1_rc, act, e), ++launches;
-        else if (nA1) k_rowblock_batch<T, X, E, true><<<nA1, kThreads, 0, s>>>(Aptr, Aidx, Aval, xin, A1_it, Ae1_it, act, e), ++launches;
+    void spmv_A(const X* xin, const E& e, const int* act, bool programmatic = false) {
+        if (thread1[0] && nA1r)
+            launch(k_rowthread_batch<T, X, E>, (nA1r + 7) / 8, programmatic, nA1r, (const int*)Aptr, (const int*)Aidx,
+                   (const T*)Aval, xin, (const int4*)A1_rc, (const int4*)Ae1_rc, act, e);
+        else if (nA1)
+            launch(k_rowblock_batch<T, X, E, true>, nA1, programmatic, (const int*)Aptr, (const int*)Aidx,
+                   (const T*)Aval, xin, (const int4*)A1_it, (const int4*)Ae1_it, act, e);
         if (nAp) k_pack_spmv<T, X, E><<<nAp, kThreads, 0, s>>>(Aptr, Aidx, Aval, xin, A_it, Ae_it, slot_inst, act, e), ++launches;
     }
     template <class X, class E>
-    void spmv_T(const X* xin, const E& e, const int* act) {
-        if (thread1[1] && nT1r) k_rowthread_batch<T, X, E><<<(nT1r + 7) / 8, kThreads, 0, s>>>(nT1r, Tptr, Tidx, Tval, xin, T1_rc, Te1_rc, act, e), ++launches;
-        else if (nT1) k_rowblock_batch<T, X, E, true><<<nT1, kThreads, 0, s>>>(Tptr, Tidx, Tval, xin, T1_it, Te1_it, act, e), ++launches;
+    void spmv_T(const X* xin, const E& e, const int* act, bool programmatic = false) {
+        if (thread1[1] && nT1r)
+            launch(k_rowthread_batch<T, X, E>, (nT1r + 7) / 8, programmatic, nT1r, (const int*)Tptr, (const int*)Tidx,
+                   (const T*)Tval, xin, (const int4*)T1_rc, (const int4*)Te1_rc, act, e);
+        else if (nT1)
+            launch(k_rowblock_batch<T, X, E, true>, nT1, programmatic, (const int*)Tptr, (const int*)Tidx,
+                   (const T*)Tval, xin, (const int4*)T1_it, (const int4*)Te1_it, act, e);
         if (nTp) k_pack_spmv<T, X, E><<<nTp, kThreads, 0, s>>>(Tptr, Tidx, Tval, xin, T_it, Te_it, slot_inst, act, e), ++launches;
     }
     void products(const int* act) {
@@ -1018,8 +1042,8 @@ struct Batch final : BatchBase {
     void block(int steps) {
         if (nT) k_pack_xupd<T><<<nT, kThreads, 0, s>>>(T_ev, Te_ev, slot_inst, running, x, ATz, c, l, u, par, xs), ++launches;
         for (int k = 0; k < steps; ++k) {
-            spmv_A(x, EpiRow<T>{Ax, z, zs, rl, ru, par}, running);
-            spmv_T(z, EpiCol<T>{ATz, x, xs, c, l, u, par, k + 1 < steps ? 1 : 0}, running);
+            spmv_A(x, EpiRow<T>{Ax, z, zs, rl, ru, par}, running, pdl);
+            spmv_T(z, EpiCol<T>{ATz, x, xs, c, l, u, par, k + 1 < steps ? 1 : 0}, running, pdl);
         }
         int g = (ninst + 255) / 256;
         k_advance<<<g, 256, 0, s>>>(ninst, st, steps);

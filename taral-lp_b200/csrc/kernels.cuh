@@ -463,8 +463,9 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_rowblock_batch(const i
                                                                const int* __restrict__ active, E epi) {
     using P = typename ProdT<T, X>::type;
     __shared__ RowSmem<P> sm;
+    pdl_release();
     const int4 e4 = __ldg(ext + blockIdx.x);
-    if (!active[e4.x]) return;
+    if (!active[e4.x]) return;  // the running flags change only between blocks (decision kernel), never in a phase
     const int tid = threadIdx.x;
     const int4 meta = __ldg(blk + blockIdx.x);
     const int r0 = meta.x + e4.y, nrows = meta.y & 0xffff;
@@ -488,6 +489,7 @@ __global__ void __launch_bounds__(kThreads) k_rowthread_batch(int n, const int* 
                                                               const int4* __restrict__ ext,
                                                               const int* __restrict__ active, E epi) {
     using P = typename ProdT<T, X>::type;
+    pdl_release();
     const int e = blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5);
     if (e >= n) return;
     const int4 e4 = __ldg(ext + e);
@@ -499,6 +501,7 @@ __global__ void __launch_bounds__(kThreads) k_rowthread_batch(int n, const int* 
     const typename E::Ops ops = epi.load(r + e4.y, e4.x);
     const int a = __ldg(ptr + r), b = __ldg(ptr + r + 1);
     const X* xb = xin + e4.z;
+    pdl_acquire();
     double s = 0;
     for (int k = a; k < b; ++k) s += double(mul_rn(P(__ldg(val + k)), P(gather(xb + __ldg(idx + k)))));
     epi.apply(r + e4.y, s, ops);
