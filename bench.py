@@ -599,15 +599,17 @@ def family_block(args):
                   "batched_rel_diff": abs(res[i]["objective"] - o["objective"]) / max(1.0, abs(o["objective"]))})
         oracle_rows.append(o)
         print("fp64 oracle", json.dumps(o), file=sys.stderr, flush=True)
-    lp48 = lpgen.RefineryBase(48, seed=7).instance(48)
-    t0 = time.perf_counter()
-    r48, _, _ = pdhg.solve(lp48, tol=tol, precision=pdhg.FP32, time_limit=600)
-    s48 = time.perf_counter() - t0
-    o48 = fp64_oracle(lp48)
-    refinery48 = {"m": lp48.m, "n": lp48.n, "nnz": lp48.nnz, "fp32_status": r48["status"],
-                  "fp32_iterations": r48["iterations"], "fp32_e2e_s": s48, "fp32_objective": r48["objective"],
-                  "fp64_oracle": o48,
-                  "fp32_rel_diff": abs(r48["objective"] - o48["objective"]) / max(1.0, abs(o48["objective"]))}
+    refinery48 = None
+    if args.oracle_sample > 0:  # the 48-period refinery LP: plain FP32 solve against its FP64 oracle
+        lp48 = lpgen.RefineryBase(48, seed=7).instance(48)
+        t0 = time.perf_counter()
+        r48, _, _ = pdhg.solve(lp48, tol=tol, precision=pdhg.FP32, time_limit=600)
+        s48 = time.perf_counter() - t0
+        o48 = fp64_oracle(lp48)
+        refinery48 = {"m": lp48.m, "n": lp48.n, "nnz": lp48.nnz, "fp32_status": r48["status"],
+                      "fp32_iterations": r48["iterations"], "fp32_e2e_s": s48, "fp32_objective": r48["objective"],
+                      "fp64_oracle": o48,
+                      "fp32_rel_diff": abs(r48["objective"] - o48["objective"]) / max(1.0, abs(o48["objective"]))}
     k = len(lps)
     its = [r["iterations"] for r in res]
     statuses = {}
@@ -699,7 +701,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the complete CPU run of the reference")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 run of the bench LP")
     ap.add_argument("--no-family", action="store_true", help="skip the batched family block")
-    ap.add_argument("--oracle-sample", type=int, default=4, help="family scenarios given the FP64 objective oracle")
+    ap.add_argument("--oracle-sample", type=int, default=4,
+                    help="family scenarios given the FP64 objective oracle (0: no oracle, no 48-period LP)")
     ap.add_argument("--workload", choices=["lp", "family", "warmstart", "ledger"], default="lp",
                     help="lp: the single large LP (the bench line); family: the batched scenario family; "
                          "warmstart: the learned warm start on the 24-period family; ledger: the reference's "
