@@ -1083,8 +1083,13 @@ struct Batch final : BatchBase {
         }
         BK(cudaMemcpyAsync(dout, h.data(), size_t(N) * sizeof(double), cudaMemcpyHostToDevice, s));
         k_cast<T><<<std::max(1, std::min((N + 255) / 256, 1184)), 256, 0, s>>>(N, dout, pv);
-        std::vector<int> ones(ninst, 1);
-        BK(cudaMemcpyAsync(pactive, ones.data(), ninst * sizeof(int), cudaMemcpyHostToDevice, s));
+        // One estimate per distinct matrix: instances that share a matrix share its scaled copy, its row blocks and
+        // the deterministic start vector, so their power iterations are the same numbers; only the first instance
+        // of each matrix iterates, the others take its estimate.
+        std::vector<int> rep(mats.size(), -1), first(static_cast<size_t>(ninst), 0);
+        for (int i = 0; i < ninst; ++i)
+            if (rep[size_t(mat_of[i])] < 0) rep[size_t(mat_of[i])] = i, first[size_t(i)] = 1;
+        BK(cudaMemcpyAsync(pactive, first.data(), ninst * sizeof(int), cudaMemcpyHostToDevice, s));
         BK(cudaMemsetAsync(est, 0, ninst * sizeof(double), s));
         T *a = pv, *b = pu;
         int g = (ninst + 255) / 256;
@@ -1107,6 +1112,7 @@ struct Batch final : BatchBase {
         std::vector<double> norms(ninst);
         BK(cudaMemcpyAsync(norms.data(), est, ninst * sizeof(double), cudaMemcpyDeviceToHost, s));
         BK(cudaStreamSynchronize(s));
+        for (int i = 0; i < ninst; ++i) norms[size_t(i)] = norms[size_t(rep[size_t(mat_of[i])])];
         double power_s = since(t0);
         // step sizes and state (gpu/pdhg.cu:767-781)
         std::vector<InstState> hs(ninst);
@@ -1125,6 +1131,7 @@ struct Batch final : BatchBase {
         }
         BK(cudaMemcpyAsync(st, hs.data(), ninst * sizeof(InstState), cudaMemcpyHostToDevice, s));
         BK(cudaMemcpyAsync(par, hpar.data(), hpar.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+        const std::vector<int> ones(static_cast<size_t>(ninst), 1);
         BK(cudaMemcpyAsync(running, ones.data(), ninst * sizeof(int), cudaMemcpyHostToDevice, s));
         // start point (gpu/pdhg.cu:450-458), cold or warm per instance
         k_start_x<T><<<std::max(1, std::min((N + 255) / 256, 1184)), 256, 0, s>>>(N, l, u, x, xlast, xs);

@@ -161,3 +161,15 @@ def test_batch_row_thread_kernel_fp32_medium_rows(engine_lib, monkeypatch):
     for a, c in zip(*outs):
         assert a["status"] == c["status"] == "near_optimal"
         assert rel(a["objective"], c["objective"]) < 5e-6, (a["objective"], c["objective"])
+
+
+def test_batch_power_iteration_once_per_matrix(engine_lib):
+    # instances sharing a matrix take the estimate of the first one (the power iteration runs once per distinct
+    # matrix): the same norm, bit for bit, and the same run as each instance batched alone
+    base = lpgen.RefineryBase(3, seed=11)
+    lps = [base.instance(3, p) for p in lpgen.perturbations(4, seed=2)] + [base.instance(2, None)]
+    res, _, _ = pdhg.Batch(lps, tol=1e-6, precision=pdhg.FP32, time_limit=300).solve()
+    for lp, r in zip(lps, res):
+        a = pdhg.Batch([lp], tol=1e-6, precision=pdhg.FP32, time_limit=300).solve()[0][0]
+        assert r["norm_a"] == a["norm_a"] and r["iterations"] == a["iterations"], (r["norm_a"], a["norm_a"])
+    assert len({r["norm_a"] for r in res[:4]}) == 1
