@@ -325,12 +325,19 @@ int gemm_umma(int M, int N, int K, const void* A, int lda, int a_mn, const void*
     const bool okA = a_mn ? make_map(&ma, A, K, M, lda, 64) : make_map(&ma, A, M, K, lda, TM);
     const bool okB = b_mn ? make_map(&mb, B, K, N, ldb, 64) : make_map(&mb, B, N, K, ldb, TN);
     if (!okA || !okB) return TARAL_ERR_CUDA;
-    static std::once_flag attr;
-    static cudaError_t attr_rc = cudaSuccess;
-    std::call_once(attr, [] {
-        attr_rc = cudaFuncSetAttribute(k_umma_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
-    });
-    if (attr_rc != cudaSuccess) return TARAL_ERR_CUDA;
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return TARAL_ERR_CUDA;
+    {  // the shared-memory opt-in is a per-device attribute of the kernel: set once on every device used
+        static std::mutex mu;
+        static bool configured[64] = {};
+        std::lock_guard<std::mutex> lock(mu);
+        if (!configured[dev]) {
+            if (cudaFuncSetAttribute(k_umma_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes) !=
+                cudaSuccess)
+                return TARAL_ERR_CUDA;
+            configured[dev] = true;
+        }
+    }
     GemmShape g;
     g.M = M, g.N = N, g.K = K, g.ldc = ldc, g.a_mn = a_mn, g.b_mn = b_mn;
     g.m_tiles = (M + TM - 1) / TM, g.n_tiles = (N + TN - 1) / TN;
@@ -338,8 +345,6 @@ int gemm_umma(int M, int N, int K, const void* A, int lda, int a_mn, const void*
     slices = slices > g.kb_total ? g.kb_total : slices;
     g.kb_per_slice = (g.kb_total + slices - 1) / slices;
     g.slices = (g.kb_total + g.kb_per_slice - 1) / g.kb_per_slice;  // every slice holds at least one K block
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int items = g.m_tiles * g.n_tiles * g.slices;
     k_umma_gemm<<<items < sms ? items : sms, kThreads, kSmemBytes, stream>>>(ma, mb, g, g.slices > 1 ? ws : C, err);
