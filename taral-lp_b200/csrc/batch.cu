@@ -932,8 +932,8 @@ struct Batch final : BatchBase {
 
     // ------------------------------------------------------------------ launches
     // `programmatic`: the width-1 kernels of an iteration's two phases start while their predecessor drains (they
-    // release their successor at entry and wait for their predecessor before the first gather); TARAL_PDL=0 turns
-    // it off. The wide-pack kernel always launches plainly.
+    // wait for their predecessor before the first gather and release their successor after that wait); on with
+    // TARAL_PDL=1. The wide-pack kernel always launches plainly.
     template <class K, class... Args>
     void launch(K kernel, int grid, bool programmatic, Args... args) {
         cudaLaunchConfig_t cfg = {};
@@ -945,7 +945,7 @@ struct Batch final : BatchBase {
         BK(cudaLaunchKernelEx(&cfg, kernel, args...));
         ++launches;
     }
-    bool pdl = true;
+    bool pdl = false;  // TARAL_PDL=1 (set at build)
     template <class X, class E>
     void spmv_A(const X* xin, const E& e, const int* act, bool programmatic = false) {
         if (thread1[0] && nA1r)

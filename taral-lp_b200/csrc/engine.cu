@@ -483,8 +483,8 @@ struct Engine final : EngineBase {
 
     // ------------------------------------------------------------------ SpMV-shaped launches
     // `programmatic`: launch with programmatic stream serialisation, so the kernel may start while its predecessor
-    // drains (both phase kernels release their successor at entry and wait for their predecessor before the first
-    // gather). Used for the two phase kernels of an iteration block when TARAL_PDL is not 0.
+    // drains (both phase kernels wait for their predecessor before the first gather and release their successor
+    // after that wait). Used for the two phase kernels of an iteration block when TARAL_PDL=1.
     template <class K, class... Args>
     void launch(K kernel, int grid, bool programmatic, Args... args) {
         cudaLaunchConfig_t cfg = {};
@@ -576,7 +576,7 @@ struct Engine final : EngineBase {
         CK(cudaGetLastError());
         started = true;
     }
-    bool pdl = true;  // TARAL_PDL=0: plain launches of the phase kernels (set at init)
+    bool pdl = false;  // TARAL_PDL=1: programmatic launches of the phase kernels (set at init; measured slower)
     void launch_block(int steps) {
         k_xupd<T><<<grid_for(n), 256, 0, st>>>(n, x, ATz, c, l, u, par, xs);
         for (int s = 0; s < steps; ++s) {

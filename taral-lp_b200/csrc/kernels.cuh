@@ -59,12 +59,16 @@ __device__ __forceinline__ double gather(const double* p) {
     return v;
 }
 
-// Programmatic dependent launch (sm_90+): a phase kernel lets its successor in the stream start as soon as every one
-// of its own CTAs is running (pdl_release), and waits for its predecessor grid to complete, with its memory visible,
-// before touching anything the predecessor writes (pdl_acquire). Without the launch attribute (a plain launch, or
-// the first kernel after a non-programmatic one) the wait returns at once, so every kernel may call both.
-__device__ __forceinline__ void pdl_release() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
-__device__ __forceinline__ void pdl_acquire() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+// Programmatic dependent launch (sm_90+, opt-in with TARAL_PDL=1): a phase kernel waits for its predecessor grid to
+// complete, with its memory visible, before touching anything the predecessor may write, and only then lets its own
+// successor launch (pdl_acquire). Releasing the successor only after the wait keeps the chain ordered: when a kernel
+// starts early, its predecessor has passed its own wait, so every kernel before that one has completed, and what the
+// early part reads -- its constant matrix stream and the vectors only its own phase writes -- is final. Without the
+// launch attribute (a plain launch) the wait returns at once and the release has no effect.
+__device__ __forceinline__ void pdl_acquire() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
 
 // Products rounded on their own (never fused into a following add), as the staged paths round them.
 __device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
@@ -412,7 +416,6 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_rowblock(const int* __
                                                          E epi) {
     using P = typename ProdT<T, X>::type;
     __shared__ RowSmem<P> sm;
-    pdl_release();
     if (skip) {  // a flag the predecessor may set
         pdl_acquire();
         if (*skip) return;
@@ -437,7 +440,6 @@ __global__ void __launch_bounds__(kThreads) k_rowthread(int rows, const int* __r
                                                         const X* __restrict__ xin, const int* __restrict__ skip,
                                                         E epi) {
     using P = typename ProdT<T, X>::type;
-    pdl_release();
     if (skip) {
         pdl_acquire();
         if (*skip) return;
@@ -463,7 +465,6 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_rowblock_batch(const i
                                                                const int* __restrict__ active, E epi) {
     using P = typename ProdT<T, X>::type;
     __shared__ RowSmem<P> sm;
-    pdl_release();
     const int4 e4 = __ldg(ext + blockIdx.x);
     if (!active[e4.x]) return;  // the running flags change only between blocks (decision kernel), never in a phase
     const int tid = threadIdx.x;
@@ -489,7 +490,6 @@ __global__ void __launch_bounds__(kThreads) k_rowthread_batch(int n, const int* 
                                                               const int4* __restrict__ ext,
                                                               const int* __restrict__ active, E epi) {
     using P = typename ProdT<T, X>::type;
-    pdl_release();
     const int e = blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5);
     if (e >= n) return;
     const int4 e4 = __ldg(ext + e);

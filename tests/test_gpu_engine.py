@@ -219,3 +219,26 @@ def test_device_scaling_equals_host_scaling(engine_lib, oracle_lib, precision):
         assert np.array_equal(a, narrow(sp.A[2])) and np.array_equal(at, narrow(sp.AT[2])), lp.name
         assert eng.bnorm == sp.bnorm and eng.cnorm == sp.cnorm, lp.name
         eng.close()
+
+
+@pytest.mark.parametrize("precision", [pdhg.FP64, pdhg.FP32], ids=["fp64", "fp32"])
+@pytest.mark.parametrize("case", ["packing_2000", "general_300x700", "transport_30x40"])
+def test_programmatic_launch_changes_nothing(engine_lib, oracle_lib, monkeypatch, precision, case):
+    """TARAL_PDL=1 launches the phase kernels with programmatic dependent launch. On these small grids a whole phase
+    fits the GPU at once, the case where an early release would let a kernel read vectors its predecessor's
+    predecessor is still writing: the iterates must equal the plain launches' bit for bit, through restarts."""
+    outs = []
+    for flag in ("0", "1"):
+        monkeypatch.setenv("TARAL_PDL", flag)
+        sp, eng, _ = _pair(CASES[case](), precision)
+        eng.set_steps(0.5 / sp.power_norm(200), 0.5 / sp.power_norm(200))
+        eng.start()
+        for action in ("avg", "cur", None):
+            eng.iterate(64)
+            if action:
+                eng.restart(action == "avg", 1 / 64)
+        outs.append((eng.eval_pair(1 / 64), eng.download(0, 1.0)))
+        eng.close()
+    (c0, a0), (x0, z0) = outs[0]
+    (c1, a1), (x1, z1) = outs[1]
+    assert np.array_equal(c0, c1) and np.array_equal(a0, a1) and np.array_equal(x0, x1) and np.array_equal(z0, z1)

@@ -107,3 +107,16 @@ def test_allocation_limit_hook(engine_lib):
     assert r["status"] == "near_optimal"
     res, _, _ = pdhg.Batch([lp, lp], tol=1e-6).solve()
     assert all(x["status"] == "near_optimal" and abs(x["iterations"] - r["iterations"]) <= 64 for x in res)
+
+
+def test_batch_programmatic_launch_changes_nothing(engine_lib, monkeypatch):
+    lps = _family(6, 3, seed=41)
+    outs = []
+    for flag in ("0", "1"):
+        monkeypatch.setenv("TARAL_PDL", flag)
+        b = pdhg.Batch(lps, tol=1e-6, precision=pdhg.FP32, time_limit=300)
+        outs.append(b.solve())
+        b.close()
+    (r0, x0, _), (r1, x1, _) = outs
+    assert [r["iterations"] for r in r0] == [r["iterations"] for r in r1]
+    assert all(np.array_equal(p, q) for p, q in zip(x0, x1))
