@@ -35,6 +35,7 @@ region, and the number of engine kernels launched in it.
   python bench.py --workload family [--instances 512]        the family block alone
   python bench.py --workload family --profile-blocks B       ncu capture mode of the batched engine (16 scenarios)
   python bench.py --workload warmstart [--train 512]         the learned warm start on the 24-period family
+  python bench.py --workload gemm                            the tcgen05 GEMM's TFLOP/s on the MLP's shapes
 """
 import argparse
 import json
@@ -691,6 +692,73 @@ def warmstart_arm(args):
     print(json.dumps(line))
 
 
+def gemm_arm(args):
+    """`--workload gemm`: the tcgen05 GEMM (taral_gemm_bf16_umma) on the warm-start MLP's three GEMM shapes at the
+    24-period output width (132,001) and batch 256, and on an 8192-cube, against the mma.sync GEMM
+    (taral_gemm_bf16) on the same operands: CUDA-event time per call (mean of 20 after 3 warm-ups), TFLOP/s = 2 M N K /
+    time, and the fraction of the measured dense BF16 peak."""
+    import ctypes as C
+    import torch
+    import pdhg
+    L = pdhg.lib()
+    dev = torch.device("cuda")
+    pk = ROOT / "MEASURED_PEAKS.json"
+    peak, kind = (json.loads(pk.read_text()).get("bf16_tflops"), "measured") if pk.exists() else (1590.0, "fallback")
+    if peak is None:
+        peak, kind = 1590.0, "fallback"
+    out_w, ld_w = 132001, 132008
+
+    def bf(shape):
+        return (torch.randn(shape, device=dev) * 0.1).to(torch.bfloat16)
+    cases = [  # name, M, N, K, A (tensor, ld, mn), B (tensor, ld, mn), slices, mma.sync form (ta, tb) or None
+        ("forward: Z = H W^T, last layer", 256, out_w, 512, (bf((256, 512)), 512, 0), (bf((out_w, 512)), 512, 0), 1,
+         (0, 1)),
+        ("dW = H^T dZ, last layer", 512, out_w, 256, (bf((256, 512)), 512, 1), (bf((256, ld_w)), ld_w, 1), 1, None),
+        ("dH = dZ W^T, last layer (split K)", 256, 512, out_w, (bf((256, ld_w)), ld_w, 0), (bf((out_w, 512)), 512, 1),
+         37, None),
+        ("square 8192^3", 8192, 8192, 8192, (bf((8192, 8192)), 8192, 0), (bf((8192, 8192)), 8192, 0), 1, (0, 1)),
+    ]
+    rows = []
+    for name, M, N, K, (a, lda, amn), (b, ldb, bmn), slices, mma in cases:
+        c = torch.empty((M, N), dtype=torch.float32, device=dev)
+        ws = torch.empty(max(slices, 1) * M * N if slices > 1 else 1, dtype=torch.float32, device=dev)
+        err = torch.zeros(1, dtype=torch.int32, device=dev)
+
+        def umma():
+            code = L.taral_gemm_bf16_umma(M, N, K, C.c_void_p(a.data_ptr()), lda, amn, C.c_void_p(b.data_ptr()), ldb,
+                                          bmn, C.c_void_p(c.data_ptr()), N, slices, C.c_void_p(ws.data_ptr()),
+                                          C.c_void_p(err.data_ptr()), None)
+            assert code == pdhg.OK, code
+
+        def timed(fn, reps=20):
+            for _ in range(3):
+                fn()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(reps):
+                fn()
+            e1.record()
+            torch.cuda.synchronize()
+            return e0.elapsed_time(e1) / reps * 1e-3
+        t = timed(umma)
+        assert int(err.item()) == 0
+        row = {"gemm": name, "M": M, "N": N, "K": K, "tcgen05_us": t * 1e6, "tcgen05_tflops": 2.0 * M * N * K / t / 1e12}
+        row["frac_of_peak"] = row["tcgen05_tflops"] / peak
+        if mma is not None:
+            wsz = torch.empty(1, dtype=torch.float32, device=dev)
+
+            def sync_gemm():
+                code = L.taral_gemm_bf16(M, N, K, mma[0], mma[1], C.c_void_p(a.data_ptr()), C.c_void_p(b.data_ptr()),
+                                         C.c_void_p(c.data_ptr()), 1, C.c_void_p(wsz.data_ptr()), None)
+                assert code == pdhg.OK, code
+            t2 = timed(sync_gemm, reps=5)
+            row["mma_sync_us"], row["mma_sync_tflops"] = t2 * 1e6, 2.0 * M * N * K / t2 / 1e12
+        rows.append(row)
+        print(json.dumps(row), file=sys.stderr, flush=True)
+    print(json.dumps({"workload": "gemm", "peak_bf16_tflops": peak, "peak_kind": kind, "rows": rows}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -703,7 +771,7 @@ def main():
     ap.add_argument("--no-family", action="store_true", help="skip the batched family block")
     ap.add_argument("--oracle-sample", type=int, default=4,
                     help="family scenarios given the FP64 objective oracle (0: no oracle, no 48-period LP)")
-    ap.add_argument("--workload", choices=["lp", "family", "warmstart", "ledger"], default="lp",
+    ap.add_argument("--workload", choices=["lp", "family", "warmstart", "ledger", "gemm"], default="lp",
                     help="lp: the single large LP (the bench line); family: the batched scenario family; "
                          "warmstart: the learned warm start on the 24-period family; ledger: the reference's "
                          "published PDHG workloads (both arms)")
@@ -721,6 +789,10 @@ def main():
         return
     if args.impl == "reference":
         reference_arm(args, rank, world)
+        return
+    if args.workload == "gemm":
+        if rank == 0:
+            gemm_arm(args)
         return
     if args.workload in ("family", "warmstart"):
         if rank == 0:

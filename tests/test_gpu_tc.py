@@ -63,7 +63,7 @@ def _umma(M, N, K, a_mn, b_mn, lda_pad=0, ldb_pad=0, ldc_pad=0, slices=1, seed=0
 
     def stored(X, mn, pad):  # X is (rows, K): K-major storage [rows][ld], MN-major storage [K][ld]
         S = X.T if mn else X
-        ld = S.shape[1] + pad
+        ld = (S.shape[1] + 7) // 8 * 8 + pad  # 16-byte rows, as the entry point requires
         buf = np.zeros((S.shape[0], ld))
         buf[:, :S.shape[1]] = S
         return torch.tensor(buf, dtype=torch.bfloat16, device=dev), ld
@@ -94,7 +94,7 @@ def test_gemm_umma_layouts(engine_lib, a_mn, b_mn, M, N, K):
 
 
 def test_gemm_umma_padded_strides_and_split_k(engine_lib):
-    _umma(256, 1001, 256, 1, 1, lda_pad=0, ldb_pad=7, ldc_pad=5)          # dW-shaped: both MN-major, padded dZ
+    _umma(256, 1001, 256, 1, 1, lda_pad=0, ldb_pad=8, ldc_pad=5)          # dW-shaped: both MN-major, padded dZ
     _umma(256, 512, 4096, 0, 1, lda_pad=8, ldb_pad=0, slices=9)           # dH-shaped: split K into slices
     _umma(256, 33001, 512, 0, 0)                                          # forward-shaped, ragged N
     _umma(100, 120, 1000, 1, 0, slices=64)                                # more slices than K blocks: clipped
