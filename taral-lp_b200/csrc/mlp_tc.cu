@@ -33,7 +33,8 @@ namespace tc {
 using bf16 = __nv_bfloat16;
 constexpr int TM = 128, TN = 256, TK = 64, kStages = 4;
 constexpr int kBytesA = TM * TK * 2, kBytesB = TN * TK * 2, kStageBytes = kBytesA + kBytesB;
-constexpr int kSmemBytes = kStages * kStageBytes + 1024;  // + alignment slack: 1 CTA per SM
+constexpr int kEpiFloats = 32 * 33;  // per epilogue warp: a 32 x 32 chunk of the accumulator, rows padded to 33
+constexpr int kSmemBytes = kStages * kStageBytes + 4 * kEpiFloats * 4 + 1024;  // + alignment slack: 1 CTA per SM
 constexpr uint32_t kTmemCols = 512;                        // two accumulators of 256 columns
 constexpr int kThreads = 192;
 constexpr int kSpinLimit = 1 << 24;
@@ -226,8 +227,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_umma_gemm(const __grid_constant
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;");
-            const int row = m0 + q * 32 + lane;
-            float* out = C + size_t(slice) * size_t(g.M) * g.ldc + size_t(row) * g.ldc;
+            // lane l holds row (m0 + 32 q + l) of each 32-column chunk; the chunk goes through this warp's tile in
+            // shared memory so that each store instruction writes 32 consecutive floats of one row
+            float* tile_sm = reinterpret_cast<float*>(smem_raw + pad + kStages * kStageBytes) + (warp - 2) * kEpiFloats;
+            float* out = C + size_t(slice) * size_t(g.M) * g.ldc;
 #pragma unroll 1
             for (int cb = 0; cb < TN / 32; ++cb) {
                 uint32_t r[32];
@@ -242,20 +245,16 @@ __global__ void __launch_bounds__(kThreads, 1) k_umma_gemm(const __grid_constant
                       "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
                     : "r"(taddr));
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-                const int c0 = n0 + cb * 32;
-                if (row < g.M) {
-                    if (c0 + 32 <= g.N && (g.ldc & 3) == 0) {
+                const int c0 = n0 + cb * 32, col = c0 + lane;
 #pragma unroll
-                        for (int i = 0; i < 32; i += 4)
-                            *reinterpret_cast<float4*>(out + c0 + i) =
-                                make_float4(__uint_as_float(r[i]), __uint_as_float(r[i + 1]), __uint_as_float(r[i + 2]),
-                                            __uint_as_float(r[i + 3]));
-                    } else {
-#pragma unroll
-                        for (int i = 0; i < 32; ++i)
-                            if (c0 + i < g.N) out[c0 + i] = __uint_as_float(r[i]);
-                    }
+                for (int i = 0; i < 32; ++i) tile_sm[lane * 33 + i] = __uint_as_float(r[i]);  // banks (lane + i) % 32
+                __syncwarp();
+#pragma unroll 8
+                for (int rr = 0; rr < 32; ++rr) {
+                    const int row = m0 + q * 32 + rr;
+                    if (row < g.M && col < g.N) out[size_t(row) * g.ldc + col] = tile_sm[rr * 33 + lane];
                 }
+                __syncwarp();
             }
             asm volatile("tcgen05.fence::before_thread_sync;");
             asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&acc_empty[acc])) : "memory");
