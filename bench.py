@@ -15,6 +15,9 @@ tolerance 1e-6, seeded synthetic data (seed = rank). One step = one full solve o
 Once per run on rank 0 at N = 1, after the timed region (each can be skipped by its flag):
 * fp64      -- the same LP solved with FP64 iterates (the reference's precision): device time, iterations
                against the reference's own FP64 count on this LP (--no-fp64);
+* learned   -- the learned warm start on 24-period scenarios (trained on 512 solutions the engine computes, on 128
+               held-out scenarios; batched, with the cold-start fallback) against cold batched and plain solves
+               (--no-learned);
 * family    -- the batched scenario family (512 refinery LPs of 4-48 periods) in one batched context against the
                plain single-instance engine, every status, the independent FP64 check of all answers, and an FP64
                objective oracle (this engine in FP64 to 1e-9 with a weak-duality certificate) on a stratified
@@ -422,6 +425,7 @@ def our_arm(args, rank, world, dist):
         once = world == 1  # the once-per-run blocks: rank 0 at N = 1 only
         fp64 = fp64_block(lp) if once and not args.no_fp64 else None
         family = family_block(args) if once and not args.no_family else None
+        learned = warmstart_block(512, 128, 4, args.epochs) if once and not args.no_learned else None
         cpu = None
         if once and not args.no_cpu_baseline and ref_binary().exists():
             cpu = reference_cpu_complete(lp, os.cpu_count() or 1)
@@ -452,6 +456,7 @@ def our_arm(args, rank, world, dist):
                                        "with their index/value stream, L2 flushed before each launch"}},
             "fp64": fp64,
             "family": family,
+            "learned": learned,
             "cpu_baseline": cpu,
             "gpu_launches": launches,
             "clocks": clk,
@@ -649,47 +654,59 @@ def family_arm(args):
     print(json.dumps(family_block(args)))
 
 
-def warmstart_arm(args):
-    """The learned warm start on the 24-period family: train on solutions of `--train` scenarios (seeds disjoint
-    from the evaluation seeds), then solve `--instances` held-out scenarios cold and warm (with the fallback
-    rule), all in batched contexts, and a sample of them with the plain single-instance engine."""
+def warmstart_block(train, instances, sample, epochs):
+    """The learned warm start on the 24-period family: train on solutions of `train` scenarios (seeds disjoint from
+    the evaluation seeds), then solve `instances` held-out scenarios cold and warm (with the fallback rule), all in
+    batched contexts, and `sample` of them with the plain single-instance engine from host arrays (wall time, like
+    the family block). Per-LP times of the batched runs are their solve calls' wall time divided by the count."""
     import numpy as np
     import lpgen
     import pdhg
     import warmstart as W
     T = 24
     base = lpgen.RefineryBase(T, seed=7)
-    Ptr, Pev = lpgen.perturbations(args.train, seed=100), lpgen.perturbations(args.instances, seed=999)
+    Ptr, Pev = lpgen.perturbations(train, seed=100), lpgen.perturbations(instances, seed=999)
     t0 = time.perf_counter()
     tr = [base.instance(T, p) for p in Ptr]
     ev = [base.instance(T, p) for p in Pev]
     gen_s = time.perf_counter() - t0
     outs, xs, ys, data_s = W.solve_batch(tr, tol=1e-5)
     t0 = time.perf_counter()
-    ws = W.train(Ptr, xs, ys, np.array([r["primal_weight"] for r in outs]), epochs=args.epochs)
+    ws = W.train(Ptr, xs, ys, np.array([r["primal_weight"] for r in outs]), epochs=epochs)
     train_s = time.perf_counter() - t0
     del xs, ys
     res = W.evaluate(ev, Pev, ws, tol=WORKLOAD["tol"])
-    plain = []
-    for i in range(min(args.sample, len(ev))):
+    plain, plain_it = [], []
+    for i in range(min(sample, len(ev))):
+        t0 = time.perf_counter()
         r, _, _ = pdhg.solve(ev[i], tol=WORKLOAD["tol"], precision=pdhg.FP32, time_limit=600)
-        plain.append(r["solve_s"])
+        plain.append(time.perf_counter() - t0)
+        plain_it.append(int(r["iterations"]))
     k = len(ev)
     warm_total = res["warm_s"] + res["probe_s"] + res["predict_s"]
-    line = {"metric": "time-to-1e-6 rel KKT per LP (learned warm start, batched)", "value": warm_total / k,
-            "unit": "s", "n_gpus": 1, "higher_is_better": False, "dtype": "fp32", "data": "synthetic",
-            "config": {"workload": f"refinery family, {T} periods ({ev[0].m} rows x {ev[0].n} columns), "
-                                   f"{args.train} training / {k} held-out scenarios (disjoint seeds)",
-                       "mlp": f"256 -> 512 x 3 (GELU) -> {ev[0].n + ev[0].m + 1}, bf16 weights, fp32 accumulate"},
+    plain_lp = float(np.mean(plain)) if plain else None
+    statuses = {}
+    for st in res["warm_status"]:
+        statuses[st] = statuses.get(st, 0) + 1
+    return {"metric": "time-to-1e-6 rel KKT per LP, learned warm start + batched vs the plain engine",
+            "workload": f"refinery family, {T} periods ({ev[0].m} rows x {ev[0].n} columns), {train} training / "
+                        f"{k} held-out scenarios (disjoint seeds), tol {WORKLOAD['tol']}, FP32 iterates",
+            "mlp": f"256 -> 512 x 3 (GELU) -> {ev[0].n + ev[0].m + 1}, bf16 weights, fp32 accumulate, tcgen05 GEMMs",
             "train": {"solutions_s": data_s, "train_s": train_s, "final_loss": ws.net.last_loss,
-                      "generate_s": gen_s, "epochs": args.epochs},
-            "cold": {"per_lp_s": res["cold_s"] / k, "iterations_mean": float(np.mean(res["cold_iterations"]))},
-            "warm": {"per_lp_s": warm_total / k, "iterations_mean": float(np.mean(res["warm_iterations"])),
-                     "used_warm": int(sum(res["used_warm"])), "probe_s": res["probe_s"]},
-            "plain_single_instance_per_lp_s": float(np.mean(plain)) if plain else None,
+                      "generate_s": gen_s, "epochs": epochs},
+            "cold_batched": {"per_lp_s": res["cold_s"] / k, "iterations_mean": float(np.mean(res["cold_iterations"]))},
+            "learned_batched": {"per_lp_s": warm_total / k, "iterations_mean": float(np.mean(res["warm_iterations"])),
+                                "used_warm": int(sum(res["used_warm"])), "probe_s": res["probe_s"],
+                                "predict_s": res["predict_s"], "statuses": statuses},
+            "plain_single_instance": {"per_lp_s": plain_lp, "sample": len(plain),
+                                      "iterations_mean": float(np.mean(plain_it)) if plain_it else None},
+            "speedup_learned_batched_vs_plain": None if plain_lp is None else plain_lp / (warm_total / k),
             "objective_max_rel_diff_warm_vs_cold": float(max(abs(a - b) / max(1.0, abs(a)) for a, b in
                                                              zip(res["cold_objective"], res["warm_objective"])))}
-    print(json.dumps(line))
+
+
+def warmstart_arm(args):
+    print(json.dumps(warmstart_block(args.train, args.instances, args.sample, args.epochs)))
 
 
 def gemm_arm(args):
@@ -769,6 +786,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the complete CPU run of the reference")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 run of the bench LP")
     ap.add_argument("--no-family", action="store_true", help="skip the batched family block")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned warm-start block")
     ap.add_argument("--oracle-sample", type=int, default=4,
                     help="family scenarios given the FP64 objective oracle (0: no oracle, no 48-period LP)")
     ap.add_argument("--workload", choices=["lp", "family", "warmstart", "ledger", "gemm"], default="lp",
