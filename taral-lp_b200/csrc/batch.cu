@@ -96,6 +96,7 @@ __global__ void __launch_bounds__(kThreads, 6) k_pack_spmv(const int* __restrict
                                                                      const int* __restrict__ active, E epi) {
     using P = typename ProdT<T, X>::type;
     __shared__ PackSmem<P> sm;
+    __shared__ typename E::Stage st;
     const int4 e4 = __ldg(ext + blockIdx.x);
     const int pack = e4.x, vbase = e4.y, gbase = e4.z, W = e4.w, lw = log2w(W);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, my_t = tid & (W - 1);
@@ -130,10 +131,9 @@ __global__ void __launch_bounds__(kThreads, 6) k_pack_spmv(const int* __restrict
         }
         return;
     }
-    // item tid = (row tid >> lw, slot my_t): its epilogue operands are fetched before the matrix stream
+    // item tid = (row tid >> lw, slot my_t): its epilogue operands are copied to shared memory before the matrix stream
     const bool mine = my_live && tid < (nrows << lw);
-    typename E::Ops ops{};
-    if (mine) ops = epi.load(vbase + tid, my_inst);
+    if (mine) epi.stage(vbase + tid, tid, st);
     // 1. stage the products of the block's (nonzero, slot) pairs: all index / value loads, then all gathers
     const int a0 = p0 & ~3, npairs = (p1 - a0) << lw;
     int c[kPairs];
@@ -182,7 +182,7 @@ __global__ void __launch_bounds__(kThreads, 6) k_pack_spmv(const int* __restrict
         if (lane == 0) sm.rowsum[q] = s;
     }
     __syncthreads();
-    if (mine) epi.apply(vbase + tid, sm.rowsum[tid], ops);
+    if (mine) epi.finish(vbase + tid, my_inst, tid, sm.rowsum[tid], st);
 }
 
 // Per-(CTA, slot) partial sums of the row (ROW = true) or column KKT scalars over one pack block, CTAs in

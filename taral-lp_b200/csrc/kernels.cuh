@@ -6,10 +6,12 @@
 // longer than kTile forms a block of its own). One CTA per block:
 //   1. stage  -- the block's val/idx range is read with 16-byte vector loads (scalar at the ragged ends), each
 //                nonzero's product with the gathered vector entry is written to shared memory;
-//   2. reduce -- rows are summed from shared memory by groups of G lanes (G = power of two >= the block's mean
-//                row length, 1..32) with a shuffle tree, in FP64;
+//   2. reduce -- rows are summed from shared memory in FP64: a row of at most kShort nonzeros by its own thread
+//                in entry order, a longer row by a warp (lanes strided, shuffle tree); the autotuner's row-split
+//                policies (block flags below) change this per block;
 //   3. epilogue -- one thread per row applies the fused step (prox, projection, running sums) with its operands
-//                loaded before stage 1, so their latency overlaps the matrix stream.
+//                copied asynchronously into shared memory before stage 1, so their latency overlaps the matrix
+//                stream without holding registers across it.
 // The summation order depends only on the matrix, so results are bit-reproducible run to run.
 #pragma once
 #include <cstdint>
@@ -21,7 +23,11 @@ constexpr int kThreads = 256;  // threads per CTA in every SpMV-shaped kernel
 constexpr int kTile = 2044;    // nonzeros staged per row block: with the 16-byte alignment slack, 512 quads
 constexpr int kRowsMax = 256;  // rows per row block (one epilogue row per thread)
 constexpr int kRedThreads = 256;
-constexpr int kMinBlocks = 8;   // resident CTAs per SM the SpMV kernels are compiled for (32 registers)
+// Resident CTAs per SM the row-block kernels are compiled for, by product type: 8 (32 registers) with float
+// products; 5 (48 registers) with double products, whose staging registers would otherwise spill to local memory
+// (measured on the bench LP's row phase in FP64: 55.7 us at 8 CTAs with spills, 40.2 us at 5 without).
+template <class P> constexpr int kMinBlocks = 5;
+template <> constexpr int kMinBlocks<float> = 8;
 
 template <class T>
 __device__ __forceinline__ T clampv(T v, T lo, T hi) { return v < lo ? lo : (v > hi ? hi : v); }
@@ -78,18 +84,39 @@ __device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(
 template <class T, class X> struct ProdT { using type = double; };
 template <> struct ProdT<float, float> { using type = float; };
 
+// ------------------------------------------------------------------------------------------ async copies
+// Global -> shared copies of one 4- or 8-byte element (cp.async): while in flight they hold no registers, so the
+// row-block kernels fetch a row's epilogue operands before the matrix stream without keeping them in registers
+// across it (at the 32 registers of 8 CTAs per SM, operands held in registers spill to local memory).
+__device__ __forceinline__ void copy_async(float* dst, const float* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;"
+                 :: "r"(unsigned(__cvta_generic_to_shared(dst))), "l"(src) : "memory");
+}
+__device__ __forceinline__ void copy_async(double* dst, const double* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;"
+                 :: "r"(unsigned(__cvta_generic_to_shared(dst))), "l"(src) : "memory");
+}
+__device__ __forceinline__ void copy_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void copy_async_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // ------------------------------------------------------------------------------------------ epilogues
+// Two forms of the same step:
+//   load(r, inst) -> Ops, apply(r, s, ops): the operands of row r in registers (the thread-per-row kernels);
+//   stage(r, t, st), finish(r, inst, t, s, st): the operands copied asynchronously into slot t of a shared-memory
+//     Stage before the matrix stream and consumed after the sums (the row-block kernels; t < kRowsMax).
+// inst = the row's instance in a batch, 0 otherwise; step sizes par[2 inst] = tau, par[2 inst + 1] = sigma.
 // y[r] = s
 template <class Y>
 struct EpiStore {
     Y* y;
     struct Ops {};
+    struct Stage {};
     __device__ __forceinline__ Ops load(int, int) const { return {}; }
     __device__ __forceinline__ void apply(int r, double s, const Ops&) const { y[r] = Y(s); }
+    __device__ __forceinline__ void stage(int, int, Stage&) const {}
+    __device__ __forceinline__ void finish(int r, int, int, double s, Stage&) const { y[r] = Y(s); }
 };
 
-// Epilogues: load(r, inst) fetches row r's operands before the matrix stream (inst = the row's instance in a
-// batch, 0 otherwise; step sizes par[2 inst] = tau, par[2 inst + 1] = sigma), apply(r, s, ops) consumes the sum.
 // Dual step of one row (gpu/pdhg.cu:178-190 semantics, running sum of z in FP64):
 //   v = z + sigma (2 s - Ax_old);  z = prox: v - sigma*rl if v/sigma < rl, v - sigma*ru if v/sigma > ru, else 0;
 //   Ax_old = s;  zs += z.
@@ -102,14 +129,29 @@ struct EpiRow {
     const T *rl, *ru;
     const double* par;
     struct Ops { double z, ax, rl, ru, sig, zs; };
+    struct Stage { double zs[kRowsMax]; T z[kRowsMax], ax[kRowsMax], rl[kRowsMax], ru[kRowsMax]; };
+    __device__ __forceinline__ void step(int r, double s, double z0, double ax, double lo, double hi, double sig,
+                                         double zs0) const {
+        const T st = T(s);
+        const double v = z0 + sig * (2.0 * double(st) - ax), q = v / sig;
+        const T zn = T(q < lo ? v - sig * lo : (q > hi ? v - sig * hi : 0.0));
+        Ax[r] = st, z[r] = zn, zs[r] = zs0 + double(zn);
+    }
     __device__ __forceinline__ Ops load(int r, int inst) const {
         return {double(z[r]), double(Ax[r]), double(rl[r]), double(ru[r]), par[2 * inst + 1], zs[r]};
     }
     __device__ __forceinline__ void apply(int r, double s, const Ops& o) const {
-        const T st = T(s);
-        const double sig = o.sig, v = o.z + sig * (2.0 * double(st) - o.ax), q = v / sig;
-        const T zn = T(q < o.rl ? v - sig * o.rl : (q > o.ru ? v - sig * o.ru : 0.0));
-        Ax[r] = st, z[r] = zn, zs[r] = o.zs + double(zn);
+        step(r, s, o.z, o.ax, o.rl, o.ru, o.sig, o.zs);
+    }
+    __device__ __forceinline__ void stage(int r, int t, Stage& st) const {
+        copy_async(&st.z[t], z + r), copy_async(&st.ax[t], Ax + r), copy_async(&st.rl[t], rl + r);
+        copy_async(&st.ru[t], ru + r), copy_async(&st.zs[t], zs + r);
+        copy_async_commit();
+    }
+    __device__ __forceinline__ void finish(int r, int inst, int t, double s, Stage& st) const {
+        copy_async_wait();
+        step(r, s, double(st.z[t]), double(st.ax[t]), double(st.rl[t]), double(st.ru[t]), par[2 * inst + 1],
+             st.zs[t]);
     }
 };
 
@@ -123,17 +165,36 @@ struct EpiCol {
     const double* par;
     int upd;
     struct Ops { double x, c, l, u, tau, xs; };
+    struct Stage { double xs[kRowsMax]; T x[kRowsMax], c[kRowsMax], l[kRowsMax], u[kRowsMax]; };
+    __device__ __forceinline__ void step(int r, double s, double x0, double c0, double lo, double hi, double tau,
+                                         double xs0) const {
+        const T st = T(s);
+        ATz[r] = st;
+        if (upd) {
+            const T xn = T(clampv(x0 - tau * (c0 + double(st)), lo, hi));
+            x[r] = xn, xs[r] = xs0 + double(xn);
+        }
+    }
     __device__ __forceinline__ Ops load(int r, int inst) const {
         if (!upd) return {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
         return {double(x[r]), double(c[r]), double(l[r]), double(u[r]), par[2 * inst], xs[r]};
     }
     __device__ __forceinline__ void apply(int r, double s, const Ops& o) const {
-        const T st = T(s);
-        ATz[r] = st;
-        if (upd) {
-            const T xn = T(clampv(o.x - o.tau * (o.c + double(st)), o.l, o.u));
-            x[r] = xn, xs[r] = o.xs + double(xn);
+        step(r, s, o.x, o.c, o.l, o.u, o.tau, o.xs);
+    }
+    __device__ __forceinline__ void stage(int r, int t, Stage& st) const {
+        if (!upd) return;
+        copy_async(&st.x[t], x + r), copy_async(&st.c[t], c + r), copy_async(&st.l[t], l + r);
+        copy_async(&st.u[t], u + r), copy_async(&st.xs[t], xs + r);
+        copy_async_commit();
+    }
+    __device__ __forceinline__ void finish(int r, int inst, int t, double s, Stage& st) const {
+        if (!upd) {
+            ATz[r] = T(s);
+            return;
         }
+        copy_async_wait();
+        step(r, s, double(st.x[t]), double(st.c[t]), double(st.l[t]), double(st.u[t]), par[2 * inst], st.xs[t]);
     }
 };
 
@@ -410,12 +471,13 @@ __device__ __forceinline__ void block_sums(const int* __restrict__ ptr, const in
 
 // One launch over all row blocks of one matrix; `skip` (may be NULL): return at once when *skip != 0.
 template <class T, class X, class E, bool VEC>
-__global__ void __launch_bounds__(kThreads, kMinBlocks) k_rowblock(const int* __restrict__ ptr, const int* __restrict__ idx,
+__global__ void __launch_bounds__(kThreads, kMinBlocks<typename ProdT<T, X>::type>) k_rowblock(const int* __restrict__ ptr, const int* __restrict__ idx,
                                                          const T* __restrict__ val, const X* __restrict__ xin,
                                                          const int4* __restrict__ blk, const int* __restrict__ skip,
                                                          E epi) {
     using P = typename ProdT<T, X>::type;
     __shared__ RowSmem<P> sm;
+    __shared__ typename E::Stage st;
     if (skip) {  // a flag the predecessor may set
         pdl_acquire();
         if (*skip) return;
@@ -423,11 +485,10 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_rowblock(const int* __
     const int tid = threadIdx.x;
     const int4 meta = __ldg(blk + blockIdx.x);
     const int r0 = meta.x, nrows = meta.y & 0xffff;
-    typename E::Ops ops{};
     const bool mine = tid < nrows;
-    if (mine) ops = epi.load(r0 + tid, 0);  // this phase's own vectors: the other phase does not write them
+    if (mine) epi.stage(r0 + tid, tid, st);  // this phase's own vectors: the other phase does not write them
     block_sums<T, X, VEC>(ptr, idx, val, xin, meta, sm);
-    if (mine) epi.apply(r0 + tid, sm.rowsum[tid], ops);
+    if (mine) epi.finish(r0 + tid, 0, tid, sm.rowsum[tid], st);
 }
 
 // One thread per row, its products summed in entry order: for a matrix whose rows all hold at most kShort nonzeros
@@ -458,23 +519,23 @@ __global__ void __launch_bounds__(kThreads) k_rowthread(int rows, const int* __r
 // offset, 0}: the block's rows r of the (possibly shared) matrix are rows r + shift of the concatenated instance
 // vectors, and its column indices address xin + offset. Blocks of instances with active[instance] == 0 return.
 template <class T, class X, class E, bool VEC>
-__global__ void __launch_bounds__(kThreads, kMinBlocks) k_rowblock_batch(const int* __restrict__ ptr, const int* __restrict__ idx,
+__global__ void __launch_bounds__(kThreads, kMinBlocks<typename ProdT<T, X>::type>) k_rowblock_batch(const int* __restrict__ ptr, const int* __restrict__ idx,
                                                                const T* __restrict__ val, const X* __restrict__ xin,
                                                                const int4* __restrict__ blk,
                                                                const int4* __restrict__ ext,
                                                                const int* __restrict__ active, E epi) {
     using P = typename ProdT<T, X>::type;
     __shared__ RowSmem<P> sm;
+    __shared__ typename E::Stage st;
     const int4 e4 = __ldg(ext + blockIdx.x);
     if (!active[e4.x]) return;  // the running flags change only between blocks (decision kernel), never in a phase
     const int tid = threadIdx.x;
     const int4 meta = __ldg(blk + blockIdx.x);
     const int r0 = meta.x + e4.y, nrows = meta.y & 0xffff;
-    typename E::Ops ops{};
     const bool mine = tid < nrows;
-    if (mine) ops = epi.load(r0 + tid, e4.x);
+    if (mine) epi.stage(r0 + tid, tid, st);
     block_sums<T, X, VEC>(ptr, idx, val, xin + e4.z, meta, sm);
-    if (mine) epi.apply(r0 + tid, sm.rowsum[tid], ops);
+    if (mine) epi.finish(r0 + tid, e4.x, tid, sm.rowsum[tid], st);
 }
 
 // Batched thread-per-row form: one warp per entry of a row-chunk list, chunk[e] = {first row in the concatenated
