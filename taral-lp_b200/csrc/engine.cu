@@ -221,16 +221,27 @@ struct Engine final : EngineBase {
     // only the FP64 KKT sums over rows change order. TARAL_ROWORDER=0 keeps the model's order. rperm[k] = model row
     // at position k.
     std::vector<int> rperm;
-    bool order_rows(const Csr& a, const Csr& at, Csr& ap, Csr& atp) {
+    // ap: A with its rows in that order; at_idx: A^T's row indices renumbered (its pointers and values unchanged).
+    // The copies run on the host threads.
+    bool order_rows(const Csr& a, const CsrRef& at, Csr& ap, Entries<int32_t>& at_idx) {
         rperm.clear();
         const char* e = std::getenv("TARAL_ROWORDER");  // 0 off, otherwise (default) rows sorted by length
         const int mode = e ? std::atoi(e) : 1;
         if (sizeof(T) != sizeof(float) || mode <= 0 || a.rows == 0) return false;
         const int rows = a.rows;
-        std::vector<int> perm(static_cast<size_t>(rows));
-        for (int r = 0; r < rows; ++r) perm[size_t(r)] = r;
         auto len = [&](int r) { return a.ptr[size_t(r) + 1] - a.ptr[size_t(r)]; };
-        std::stable_sort(perm.begin(), perm.end(), [&](int x, int y) { return len(x) < len(y); });
+        std::vector<int> perm(static_cast<size_t>(rows));
+        int64_t longest = 0;
+        for (int r = 0; r < rows; ++r) longest = std::max(longest, len(r));
+        if (longest <= 16 * int64_t(rows) + 1024) {  // stable counting sort by length
+            std::vector<int> at(size_t(longest) + 2, 0);
+            for (int r = 0; r < rows; ++r) at[size_t(len(r)) + 1]++;
+            for (size_t l = 1; l < at.size(); ++l) at[l] += at[l - 1];
+            for (int r = 0; r < rows; ++r) perm[size_t(at[size_t(len(r))]++)] = r;
+        } else {
+            for (int r = 0; r < rows; ++r) perm[size_t(r)] = r;
+            std::stable_sort(perm.begin(), perm.end(), [&](int x, int y) { return len(x) < len(y); });
+        }
         int split = 0;
         while (split < rows && len(perm[size_t(split)]) <= kShort) ++split;
         if (split == rows || split == 0) return false;  // rows of one kind: nothing to separate
@@ -238,16 +249,27 @@ struct Engine final : EngineBase {
         for (int k = 0; k < rows; ++k) inv[size_t(perm[size_t(k)])] = k;
         ap.rows = rows;
         ap.ptr.assign(size_t(rows) + 1, 0);
+        for (int k = 0; k < rows; ++k) ap.ptr[size_t(k) + 1] = ap.ptr[size_t(k)] + len(perm[size_t(k)]);
         ap.idx.resize(a.idx.size()), ap.val.resize(a.val.size());
-        for (int k = 0; k < rows; ++k) {
-            const int64_t b = a.ptr[size_t(perm[size_t(k)])], l = len(perm[size_t(k)]), o = ap.ptr[size_t(k)];
-            std::copy(a.idx.begin() + b, a.idx.begin() + b + l, ap.idx.begin() + o);
-            std::copy(a.val.begin() + b, a.val.begin() + b + l, ap.val.begin() + o);
-            ap.ptr[size_t(k) + 1] = o + l;
-        }
-        atp.rows = at.rows, atp.ptr = at.ptr, atp.val = at.val;
-        atp.idx.resize(at.idx.size());
-        for (size_t q = 0; q < at.idx.size(); ++q) atp.idx[q] = inv[size_t(at.idx[q])];
+        const int threads = host_threads();
+        const int64_t nnz = ap.ptr[size_t(rows)];
+        split_ranges(threads, threads, [&](int, int64_t q0, int64_t q1) {  // rows cut into ranges of equal nonzeros
+            for (int64_t q = q0; q < q1; ++q) {
+                const auto row_at = [&](int64_t e) {
+                    return int(std::lower_bound(ap.ptr.begin(), ap.ptr.end(), e) - ap.ptr.begin());
+                };
+                const int k0 = row_at(nnz * q / threads), k1 = q + 1 == threads ? rows : row_at(nnz * (q + 1) / threads);
+                for (int k = k0; k < k1; ++k) {
+                    const int64_t b = a.ptr[size_t(perm[size_t(k)])], l = len(perm[size_t(k)]), o = ap.ptr[size_t(k)];
+                    std::copy(a.idx.begin() + b, a.idx.begin() + b + l, ap.idx.begin() + o);
+                    std::copy(a.val.begin() + b, a.val.begin() + b + l, ap.val.begin() + o);
+                }
+            }
+        });
+        at_idx.resize(size_t(at.nnz()));
+        split_ranges(at.nnz(), threads, [&](int, int64_t q0, int64_t q1) {
+            for (int64_t q = q0; q < q1; ++q) at_idx[size_t(q)] = inv[size_t(at.idx[q])];
+        });
         rperm = std::move(perm);
         return true;
     }
@@ -262,17 +284,17 @@ struct Engine final : EngineBase {
         return o;
     }
     // Row pointers, column indices and row blocks of one matrix on the device; the values are left to the caller.
-    DevMat upload_structure(const Csr& a) {
+    DevMat upload_structure(const CsrRef& a) {
         DevMat d;
-        d.rows = a.rows, d.nnz = int64_t(a.idx.size());
+        d.rows = a.rows, d.nnz = a.nnz();
         std::vector<int> p32(size_t(a.rows) + 1);
         for (int r = 0; r <= a.rows; ++r) p32[r] = int(a.ptr[r]);
         for (int r = 0; r < a.rows; ++r) d.maxrow = std::max(d.maxrow, p32[r + 1] - p32[r]);
-        std::vector<int4> blk = build_row_blocks(a.ptr.data(), a.rows);
+        std::vector<int4> blk = build_row_blocks(a.ptr, a.rows);
         d.nblk = int(blk.size());
         d.ptr = alloc<int>(p32.size()), d.idx = alloc<int>(size_t(d.nnz)), d.blk = alloc<int4>(blk.size());
         CK(cudaMemcpyAsync(d.ptr, p32.data(), p32.size() * sizeof(int), cudaMemcpyHostToDevice, st));
-        if (d.nnz) CK(cudaMemcpyAsync(d.idx, a.idx.data(), size_t(d.nnz) * sizeof(int), cudaMemcpyHostToDevice, st));
+        if (d.nnz) CK(cudaMemcpyAsync(d.idx, a.idx, size_t(d.nnz) * sizeof(int), cudaMemcpyHostToDevice, st));
         if (!blk.empty())
             CK(cudaMemcpyAsync(d.blk, blk.data(), blk.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
         d.val = alloc<T>(size_t(d.nnz));
@@ -286,13 +308,15 @@ struct Engine final : EngineBase {
     void init_model(const taral_model& md, double sign, Scaled& P, int freq, unsigned flags, double* host_s) {
         auto t0 = Clock::now();
         Csr hA, hAT;
-        model_matrices(md, hA, hAT);
+        const CsrRef mAT = model_matrices_ref(md, hA, hAT);  // A^T: the model's own arrays when they are A^T
         // FP32: rows in ascending length internally (rperm: internal -> model row); A^T keeps its entry order (its
         // indices renumbered), so both phases sum exactly as before
-        Csr hAp, hATp;
-        const bool reorder = order_rows(hA, hAT, hAp, hATp);
-        const Csr& uA = reorder ? hAp : hA;
-        const Csr& uAT = reorder ? hATp : hAT;
+        Csr hAp;
+        Entries<int32_t> at_idx;
+        const bool reorder = order_rows(hA, mAT, hAp, at_idx);
+        const CsrRef uA = ref(reorder ? hAp : hA);
+        CsrRef uAT = mAT;
+        if (reorder) uAT.idx = at_idx.data();
         double hs = since(t0);
         begin(md.m, md.n, freq, flags);
         A = upload_structure(uA), AT = upload_structure(uAT);
@@ -319,8 +343,8 @@ struct Engine final : EngineBase {
         }
         dr = scratch(size_t(m)), dc = scratch(size_t(n)), rs = scratch(size_t(m)), cs = scratch(size_t(n));
         if (nz) {
-            CK(cudaMemcpyAsync(va, uA.val.data(), size_t(nz) * sizeof(double), cudaMemcpyHostToDevice, st));
-            CK(cudaMemcpyAsync(vt, uAT.val.data(), size_t(nz) * sizeof(double), cudaMemcpyHostToDevice, st));
+            CK(cudaMemcpyAsync(va, uA.val, size_t(nz) * sizeof(double), cudaMemcpyHostToDevice, st));
+            CK(cudaMemcpyAsync(vt, uAT.val, size_t(nz) * sizeof(double), cudaMemcpyHostToDevice, st));
         }
         scale_on_device(m, n, A.ptr, A.idx, va, AT.ptr, AT.idx, vt, dr, dc, rs, cs, st);
         if (sizeof(T) != sizeof(double) && nz) {
@@ -335,7 +359,7 @@ struct Engine final : EngineBase {
         }  // FP64 scratch released
         t0 = Clock::now();
         if (reorder) P.Dr = to_model(P.Dr);
-        hAp = Csr(), hATp = Csr();
+        hAp = Csr(), at_idx = Entries<int32_t>();
         P.A = std::move(hA), P.AT = Csr();  // the unscaled row-wise copy serves the original-space check
         P.a_original = true;
         hAT = Csr();

@@ -7,7 +7,10 @@
 #include <cstdio>
 #include <limits>
 #include <stdexcept>
+#include <memory>
 #include <string>
+#include <thread>
+#include <utility>
 #include <vector>
 
 #include "../../include/taral_pdhg.h"
@@ -39,17 +42,62 @@ struct ParseError : std::runtime_error {
 };
 Model read_mps(const std::string& path);  // src/mps.cpp:388-399 semantics
 
+// Allocator whose value-less construct leaves trivially constructible elements uninitialised: resize() of an entry
+// array that is written in full right after, by several threads, does not first zero (and page in) all of it on one
+// thread.
+template <class T>
+struct NoInit : std::allocator<T> {
+    template <class U>
+    struct rebind {
+        using other = NoInit<U>;
+    };
+    NoInit() = default;
+    template <class U>
+    NoInit(const NoInit<U>&) noexcept {}
+    template <class U>
+    void construct(U* p) noexcept {
+        ::new (static_cast<void*>(p)) U;
+    }
+    template <class U, class... A>
+    void construct(U* p, A&&... a) {
+        ::new (static_cast<void*>(p)) U(std::forward<A>(a)...);
+    }
+};
+template <class T>
+using Entries = std::vector<T, NoInit<T>>;
+
 // Row-wise CSR (gpu/pdhg.cu:49-53), int64 row pointers.
 struct Csr {
     int rows = 0;
     std::vector<int64_t> ptr;
-    std::vector<int32_t> idx;
-    std::vector<double> val;
+    Entries<int32_t> idx;
+    Entries<double> val;
     taral_csr view(int cols) const { return {rows, cols, int64_t(val.size()), ptr.data(), idx.data(), val.data()}; }
 };
-// Transpose of the CSR given by (ptr, idx, val) (gpu/pdhg.cu:55-70), the scatter on `threads` threads.
+// A row-wise matrix held elsewhere (a Csr, or the column-wise arrays of a model read as its transpose): ptr[0] = 0,
+// the entries of row r are [ptr[r], ptr[r + 1]).
+struct CsrRef {
+    int rows = 0;
+    const int64_t* ptr = nullptr;
+    const int32_t* idx = nullptr;
+    const double* val = nullptr;
+    int64_t nnz() const { return ptr ? ptr[rows] : 0; }
+};
+inline CsrRef ref(const Csr& a) { return {a.rows, a.ptr.data(), a.idx.data(), a.val.data()}; }
+// Transpose of the CSR given by (ptr, idx, val) (gpu/pdhg.cu:55-70), counted and scattered on `threads` threads.
 Csr transpose_par(const int64_t* ptr, const int32_t* idx, const double* val, int rows, int cols, int threads);
 int host_threads();
+// work(q, begin, end) over [0, count) cut into `parts` contiguous ranges of about equal length, range 0 on the
+// calling thread and every other one on a thread of its own.
+template <class F>
+void split_ranges(int64_t count, int parts, F work) {
+    parts = int(std::max<int64_t>(1, std::min<int64_t>(parts, count)));
+    std::vector<std::thread> pool;
+    for (int q = 1; q < parts; ++q)
+        pool.emplace_back([&work, q, count, parts] { work(q, count * q / parts, count * (q + 1) / parts); });
+    work(0, int64_t(0), count / parts);
+    for (std::thread& t : pool) t.join();
+}
 
 // Scaled problem (gpu/pdhg.cu:72-78): A_s = diag(Dr) A diag(Dc).
 struct Scaled {
@@ -66,6 +114,9 @@ void scale_vectors(const taral_model& md, double sign, const std::vector<double>
 // The unscaled A (the transpose of the column-wise model with explicit zeros dropped) and A^T (the transpose of A):
 // the structure and entry order the reference's scaling works on (gpu/pdhg.cu:80-90, 131), before any scaling.
 void model_matrices(const taral_model& md, Csr& A, Csr& AT, int threads = 0);  // threads <= 0: host_threads()
+// The same, except that when the model's columns already are A^T (rows ascending in every column, no explicit
+// zero) AT is left empty and the result refers to the model's own arrays; otherwise it refers to AT.
+CsrRef model_matrices_ref(const taral_model& md, Csr& A, Csr& AT, int threads = 0);
 
 struct Options {  // gpu/pdhg.cu:744-750
     double tol = 1e-4, time_limit = 3600;

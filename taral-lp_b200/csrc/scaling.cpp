@@ -9,40 +9,55 @@
 
 namespace taral {
 
-// CSR transpose by counting sort (gpu/pdhg.cu:55-70 semantics: rows of the output ascending), the scatter split
-// over threads by ranges of output rows: every thread reads the whole input in order and writes only its own rows,
-// so each output row is filled in the sequential order and the result does not depend on the thread count.
+// CSR transpose by counting sort (gpu/pdhg.cu:55-70 semantics: rows of the output ascending). The input rows are
+// cut into ranges of about equal nonzeros, one per thread; every range counts its entries per output row, each
+// range's entries of an output row follow those of the ranges before it, and every range scatters its own entries:
+// each output row is filled in the sequential order, so the result does not depend on the thread count.
 Csr transpose_par(const int64_t* ptr, const int32_t* idx, const double* val, int rows, int cols, int threads) {
     Csr t;
     t.rows = cols;
     const int64_t nnz = ptr[rows] - ptr[0];
     t.ptr.assign(size_t(cols) + 1, 0);
-    for (int64_t k = ptr[0]; k < ptr[rows]; ++k) t.ptr[size_t(idx[k]) + 1]++;
-    for (int j = 0; j < cols; ++j) t.ptr[j + 1] += t.ptr[j];
     t.idx.resize(size_t(nnz));
     t.val.resize(size_t(nnz));
-    threads = int(std::max<int64_t>(1, std::min<int64_t>(threads, nnz / 65536)));
-    std::vector<int> cut(size_t(threads) + 1, cols);  // output rows [cut[q], cut[q+1]) belong to thread q
+    const int parts = int(std::max<int64_t>(1, std::min<int64_t>(threads, nnz / 65536)));
+    std::vector<int> cut(size_t(parts) + 1, rows);  // input rows [cut[q], cut[q+1]) form range q
     cut[0] = 0;
-    for (int q = 1; q < threads; ++q)
-        cut[q] = int(std::lower_bound(t.ptr.begin(), t.ptr.end(), nnz * q / threads) - t.ptr.begin());
-    for (int q = 1; q <= threads; ++q) cut[q] = std::max(cut[q], cut[q - 1]);
-    auto work = [&](int q) {
-        const int lo = cut[q], hi = cut[q + 1];
-        if (lo >= hi) return;
-        std::vector<int64_t> pos(t.ptr.begin() + lo, t.ptr.begin() + hi);
-        for (int i = 0; i < rows; ++i)
-            for (int64_t k = ptr[i]; k < ptr[i + 1]; ++k) {
-                const int j = idx[k];
-                if (j < lo || j >= hi) continue;
-                const int64_t p = pos[j - lo]++;
-                t.idx[p] = i, t.val[p] = val[k];
+    for (int q = 1; q < parts; ++q)
+        cut[q] = int(std::lower_bound(ptr, ptr + rows + 1, ptr[0] + nnz * q / parts) - ptr);
+    for (int q = 1; q <= parts; ++q) cut[q] = std::max(cut[q], cut[q - 1]);
+    // slot[q][j]: range q's count of output row j, then the offset of its first entry inside that row
+    std::vector<std::vector<int32_t>> slot(static_cast<size_t>(parts));
+    split_ranges(parts, parts, [&](int, int64_t q0, int64_t q1) {
+        for (int64_t q = q0; q < q1; ++q) {
+            std::vector<int32_t>& c = slot[size_t(q)];
+            c.assign(size_t(cols), 0);
+            for (int64_t k = ptr[cut[q]]; k < ptr[cut[q + 1]]; ++k) c[size_t(idx[k])]++;
+        }
+    });
+    split_ranges(cols, threads, [&](int, int64_t j0, int64_t j1) {
+        for (int64_t j = j0; j < j1; ++j) {
+            int32_t run = 0;
+            for (int q = 0; q < parts; ++q) {
+                const int32_t c = slot[size_t(q)][size_t(j)];
+                slot[size_t(q)][size_t(j)] = run;
+                run += c;
             }
-    };
-    std::vector<std::thread> pool;
-    for (int q = 1; q < threads; ++q) pool.emplace_back(work, q);
-    work(0);
-    for (auto& th : pool) th.join();
+            t.ptr[size_t(j) + 1] = run;
+        }
+    });
+    for (int j = 0; j < cols; ++j) t.ptr[size_t(j) + 1] += t.ptr[size_t(j)];
+    split_ranges(parts, parts, [&](int, int64_t q0, int64_t q1) {
+        for (int64_t q = q0; q < q1; ++q) {
+            std::vector<int32_t>& c = slot[size_t(q)];
+            for (int i = cut[q]; i < cut[q + 1]; ++i)
+                for (int64_t k = ptr[i]; k < ptr[i + 1]; ++k) {
+                    const int j = idx[k];
+                    const int64_t p = t.ptr[size_t(j)] + c[size_t(j)]++;
+                    t.idx[size_t(p)] = i, t.val[size_t(p)] = val[k];
+                }
+        }
+    });
     return t;
 }
 
@@ -51,11 +66,21 @@ int host_threads() {
     return int(std::max(1u, std::min(h, 16u)));
 }
 
-void model_matrices(const taral_model& md, Csr& A, Csr& AT, int threads) {
+CsrRef model_matrices_ref(const taral_model& md, Csr& A, Csr& AT, int threads) {
     if (threads <= 0) threads = host_threads();
-    const int64_t k0 = md.col_ptr[0], k1 = md.col_ptr[md.n];
-    bool zeros = false;
-    for (int64_t k = k0; k < k1 && !zeros; ++k) zeros = md.val[k] == 0;
+    const int64_t k0 = md.col_ptr[0];
+    // explicit zeros and the row order inside the columns, checked over column ranges in parallel
+    std::vector<char> zero(size_t(threads), 0), unsorted(size_t(threads), 0);
+    split_ranges(md.n, threads, [&](int q, int64_t j0, int64_t j1) {
+        bool z = false, u = false;
+        for (int64_t j = j0; j < j1 && !z; ++j)
+            for (int64_t k = md.col_ptr[j]; k < md.col_ptr[j + 1]; ++k) {
+                z = z || md.val[k] == 0;
+                u = u || (k > md.col_ptr[j] && md.row_idx[k - 1] >= md.row_idx[k]);
+            }
+        zero[size_t(q)] = z, unsorted[size_t(q)] = u;
+    });
+    const bool zeros = std::find(zero.begin(), zero.end(), 1) != zero.end();
     if (!zeros) {
         A = transpose_par(md.col_ptr, md.row_idx, md.val, md.n, md.m, threads);
     } else {  // drop explicit zeros first (the column-wise copy the reference builds)
@@ -69,19 +94,30 @@ void model_matrices(const taral_model& md, Csr& A, Csr& AT, int threads) {
         }
         A = transpose_par(T.ptr.data(), T.idx.data(), T.val.data(), md.n, md.m, threads);
     }
-    // A^T = transpose(A) has ascending row indices in every column; a model whose columns already list their rows
+    // A^T = transpose(A) has ascending row indices in every column: a model whose columns already list their rows
     // in ascending order with no explicit zero is that matrix as it stands
-    bool sorted = !zeros;
-    for (int j = 0; j < md.n && sorted; ++j)
-        for (int64_t k = md.col_ptr[j] + 1; k < md.col_ptr[j + 1] && sorted; ++k) sorted = md.row_idx[k - 1] < md.row_idx[k];
+    const bool sorted = !zeros && std::find(unsorted.begin(), unsorted.end(), 1) == unsorted.end();
+    AT = Csr();
+    if (sorted && k0 == 0) return {md.n, md.col_ptr, md.row_idx, md.val};
     if (sorted) {
         AT.rows = md.n;
         AT.ptr.assign(md.col_ptr, md.col_ptr + md.n + 1);
         for (int64_t& v : AT.ptr) v -= k0;
-        AT.idx.assign(md.row_idx + k0, md.row_idx + k1);
-        AT.val.assign(md.val + k0, md.val + k1);
+        AT.idx.assign(md.row_idx + k0, md.row_idx + md.col_ptr[md.n]);
+        AT.val.assign(md.val + k0, md.val + md.col_ptr[md.n]);
     } else {
         AT = transpose_par(A.ptr.data(), A.idx.data(), A.val.data(), md.m, md.n, threads);
+    }
+    return ref(AT);
+}
+
+void model_matrices(const taral_model& md, Csr& A, Csr& AT, int threads) {
+    const CsrRef at = model_matrices_ref(md, A, AT, threads);
+    if (at.ptr == md.col_ptr) {  // the model's own arrays: copied
+        AT.rows = md.n;
+        AT.ptr.assign(at.ptr, at.ptr + md.n + 1);
+        AT.idx.assign(at.idx, at.idx + at.nnz());
+        AT.val.assign(at.val, at.val + at.nnz());
     }
 }
 
