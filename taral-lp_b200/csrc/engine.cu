@@ -213,13 +213,13 @@ struct Engine final : EngineBase {
         nnz = hA.nnz;
         finish_init(hc_ptr, hl, hu, hrl_ptr, hru_ptr, hDr, hDc);
     }
-    // Internal row order (FP32 contexts built from a model whose rows are of both kinds, short (<= kShort nonzeros)
+    // Internal row order (contexts built from a model whose rows are of both kinds, short (<= kShort nonzeros)
     // and long): rows sorted by ascending length (stable). The row phase's blocks then hold rows of similar length,
     // and the column phase's gathers of z concentrate on a contiguous tail (a long row of A is gathered by many
     // columns), which L1 and L2 serve far better. Every row's entries keep their order and A^T's entries keep
     // theirs (renumbered), so both phases add the same products in the same order as in the model's row order;
-    // only the FP64 KKT sums over rows change order. TARAL_ROWORDER=0 keeps the model's order. rperm[k] = model row
-    // at position k.
+    // only the FP64 KKT sums over rows change order (in FP64 runs the reference's iteration counts hold: the
+    // parity tests pin them). TARAL_ROWORDER=0 keeps the model's order. rperm[k] = model row at position k.
     std::vector<int> rperm;
     // ap: A with its rows in that order; at_idx: A^T's row indices renumbered (its pointers and values unchanged).
     // The copies run on the host threads.
@@ -227,7 +227,7 @@ struct Engine final : EngineBase {
         rperm.clear();
         const char* e = std::getenv("TARAL_ROWORDER");  // 0 off, otherwise (default) rows sorted by length
         const int mode = e ? std::atoi(e) : 1;
-        if (sizeof(T) != sizeof(float) || mode <= 0 || a.rows == 0) return false;
+        if (mode <= 0 || a.rows == 0) return false;
         const int rows = a.rows;
         auto len = [&](int r) { return a.ptr[size_t(r) + 1] - a.ptr[size_t(r)]; };
         std::vector<int> perm(static_cast<size_t>(rows));
@@ -309,7 +309,7 @@ struct Engine final : EngineBase {
         auto t0 = Clock::now();
         Csr hA, hAT;
         const CsrRef mAT = model_matrices_ref(md, hA, hAT);  // A^T: the model's own arrays when they are A^T
-        // FP32: rows in ascending length internally (rperm: internal -> model row); A^T keeps its entry order (its
+        // rows in ascending length internally (rperm: internal -> model row); A^T keeps its entry order (its
         // indices renumbered), so both phases sum exactly as before
         Csr hAp;
         Entries<int32_t> at_idx;
