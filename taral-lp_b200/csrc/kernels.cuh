@@ -615,6 +615,8 @@ __device__ __forceinline__ void reduce_finish(double (&v)[K], double* part, unsi
     }
 }
 
+constexpr int kEvalBatch = 4;  // elements whose loads a KKT-evaluation thread issues before summing them
+
 // Weight of row i in the per-row relative residual (gpu/pdhg.cu:138-144).
 __device__ __forceinline__ double row_rel_weight(double lo, double up, double dr) {
     double b = 0;
@@ -631,16 +633,32 @@ __global__ void __launch_bounds__(kRedThreads) k_eval_row(int m, double f, const
                                                           const T* __restrict__ zlast, double* part,
                                                           unsigned* ticket, double* out) {
     double v[5] = {0, 0, 0, 0, 0};
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
-        double ax = double(Ax[i]) * f, zz = double(z[i]) * f, lo = rl[i], up = ru[i];
-        double r = ax < lo ? lo - ax : (ax > up ? ax - up : 0), ro = r / double(Dr[i]);
-        double rr = ro * row_rel_weight(lo, up, double(Dr[i]));
+    auto add = [&](double ax, double zz, double lo, double up, double dr, double zl) {
+        ax *= f, zz *= f;
+        double r = ax < lo ? lo - ax : (ax > up ? ax - up : 0), ro = r / dr;
+        double rr = ro * row_rel_weight(lo, up, dr);
         v[0] += r * r, v[1] += ro * ro, v[2] += rr * rr;
         if (zz > 0 && up < INFINITY) v[3] -= zz * up;
         if (zz < 0 && lo > -INFINITY) v[3] -= zz * lo;
-        double dz = zz - double(zlast[i]);
+        double dz = zz - zl;
         v[4] += dz * dz;
+    };
+    // each thread takes rows i, i + G, i + 2G, ... (G = the grid's threads) in that order; the loads of kEvalBatch
+    // rows are issued before their sums, which keep the same order
+    const int G = gridDim.x * blockDim.x;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    for (; i + (kEvalBatch - 1) * G < m; i += kEvalBatch * G) {
+        double a[kEvalBatch], zz[kEvalBatch], lo[kEvalBatch], up[kEvalBatch], dr[kEvalBatch], zl[kEvalBatch];
+#pragma unroll
+        for (int e = 0; e < kEvalBatch; ++e) {
+            const int k = i + e * G;
+            a[e] = double(Ax[k]), zz[e] = double(z[k]), lo[e] = rl[k], up[e] = ru[k], dr[e] = double(Dr[k]);
+            zl[e] = double(zlast[k]);
+        }
+#pragma unroll
+        for (int e = 0; e < kEvalBatch; ++e) add(a[e], zz[e], lo[e], up[e], dr[e], zl[e]);
     }
+    for (; i < m; i += G) add(double(Ax[i]), double(z[i]), rl[i], ru[i], double(Dr[i]), double(zlast[i]));
     reduce_finish<5>(v, part, ticket, out);
 }
 
@@ -652,8 +670,9 @@ __global__ void __launch_bounds__(kRedThreads) k_eval_col(int n, double f, const
                                                           const T* __restrict__ Dc, const T* __restrict__ xlast,
                                                           double* part, unsigned* ticket, double* out) {
     double v[5] = {0, 0, 0, 0, 0};
-    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
-        double xx = double(x[j]) * f, cj = c[j], d = cj + double(ATz[j]) * f, lo = l[j], up = u[j], res = 0;
+    auto add = [&](double xx, double cj, double atz, double lo, double up, double dc, double xl) {
+        xx *= f;
+        double d = cj + atz * f, res = 0;
         v[2] += cj * xx;
         if (d > 0) {
             if (lo > -INFINITY) v[3] += d * lo;
@@ -662,9 +681,24 @@ __global__ void __launch_bounds__(kRedThreads) k_eval_col(int n, double f, const
             if (up < INFINITY) v[3] += d * up;
             else res = -d;
         }
-        double ro = res / double(Dc[j]), dx = xx - double(xlast[j]);
+        double ro = res / dc, dx = xx - xl;
         v[0] += res * res, v[1] += ro * ro, v[4] += dx * dx;
+    };
+    const int G = gridDim.x * blockDim.x;  // columns j, j + G, ... in that order, loads batched as in k_eval_row
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    for (; j + (kEvalBatch - 1) * G < n; j += kEvalBatch * G) {
+        double xx[kEvalBatch], cj[kEvalBatch], atz[kEvalBatch], lo[kEvalBatch], up[kEvalBatch], dc[kEvalBatch],
+            xl[kEvalBatch];
+#pragma unroll
+        for (int e = 0; e < kEvalBatch; ++e) {
+            const int k = j + e * G;
+            xx[e] = double(x[k]), cj[e] = c[k], atz[e] = double(ATz[k]), lo[e] = l[k], up[e] = u[k];
+            dc[e] = double(Dc[k]), xl[e] = double(xlast[k]);
+        }
+#pragma unroll
+        for (int e = 0; e < kEvalBatch; ++e) add(xx[e], cj[e], atz[e], lo[e], up[e], dc[e], xl[e]);
     }
+    for (; j < n; j += G) add(double(x[j]), c[j], double(ATz[j]), l[j], u[j], double(Dc[j]), double(xlast[j]));
     reduce_finish<5>(v, part, ticket, out);
 }
 
