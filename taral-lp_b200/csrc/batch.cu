@@ -556,6 +556,9 @@ struct Batch final : BatchBase {
 
     void build(const taral_model* md, int count, const Options& o) {
         ninst = count, opt = o, freq = std::max(1, o.eval_freq);
+        const auto tb = Clock::now();
+        std::vector<std::pair<const char*, double>> marks;  // TARAL_TIMING: set-up steps, seconds since tb
+        auto mark = [&](const char* what) { marks.emplace_back(what, since(tb)); };
         int dev = 0;
         BK(cudaGetDevice(&dev));
         keep_pool_memory(dev);
@@ -600,6 +603,7 @@ struct Batch final : BatchBase {
             same_arrays[akey] = mat_of[i];
         }
         distinct = int(mats.size());
+        mark("match");
         // 2. unscaled matrices (host transposes, threads over matrices); scaled on the device in step 3
         unsigned hw = std::max(1u, std::thread::hardware_concurrency());
         auto par_for = [&](int n, auto&& fn) {
@@ -618,6 +622,7 @@ struct Batch final : BatchBase {
             model_matrices(mk, sh.S.A, sh.S.AT, 1);
             sh.S.m = mk.m, sh.S.n = mk.n, sh.nnz = int64_t(sh.S.A.idx.size());
         });
+        mark("transposes");
         // 3. concatenated matrices (int32 offsets), uploaded unscaled and scaled on the device (scaling.cuh:
         //    bit-identical to the reference's host scaling), values narrowed to T in place
         std::vector<int> hAptr, hTptr;
@@ -686,6 +691,7 @@ struct Batch final : BatchBase {
                 }
             }
         }
+        mark("upload+scaling");
         vecs.resize(count);
         par_for(count, [&](int i) {
             const Shared& sh = *mats[mat_of[i]];
@@ -830,7 +836,14 @@ struct Batch final : BatchBase {
         for (int i = 0; i < count; ++i) nnz_total += mats[mat_of[i]]->nnz;
         models.clear();
         for (int i = 0; i < count; ++i) models.push_back(md + i);
+        mark("vectors+lists");
         tune();
+        mark("tune");
+        if (std::getenv("TARAL_TIMING")) {
+            std::fprintf(stderr, "taral: batch set-up");
+            for (const auto& mk : marks) std::fprintf(stderr, " %s %.3f", mk.first, mk.second);
+            std::fprintf(stderr, " s\n");
+        }
     }
 
     // Autotuner, per phase over the whole batch (batches of at least 2^20 nonzeros), timed on the phase itself with
@@ -1228,6 +1241,7 @@ struct Batch final : BatchBase {
         BK(cudaEventElapsedTime(&ms, e0, e1));
         cudaEventDestroy(e0), cudaEventDestroy(e1);
         double solve_s = since(t0);
+        const auto tf = Clock::now();
         // original-space check of every instance (independent: spread over the host threads)
         std::atomic<int> next{0};
         auto finish_one = [&](int i) {
@@ -1262,6 +1276,9 @@ struct Batch final : BatchBase {
                 for (int i = next++; i < ninst; i = next++) finish_one(i);
             });
         for (auto& th : pool) th.join();
+        if (std::getenv("TARAL_TIMING"))
+            std::fprintf(stderr, "taral: batch solve: power %.3f s, to the download %.3f s, check %.3f s, device %.3f s\n",
+                         power_s, solve_s, since(tf), ms * 1e-3);
         __atomic_store_n(h_cancel, 0, __ATOMIC_SEQ_CST);  // a request applies to one solve
         for (int i = 0; i < ninst; ++i)
             if (fin[size_t(i)].status == TARAL_CANCELLED) return TARAL_ERR_CANCELLED;
