@@ -564,43 +564,54 @@ struct Batch final : BatchBase {
         keep_pool_memory(dev);
         BK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
         if (const char* e = std::getenv("TARAL_PDL")) pdl = std::atoi(e) != 0;
-        // 1. distinct matrices (same sizes and identical col_ptr / row_idx / val)
-        std::map<std::pair<uint64_t, std::pair<int, int>>, int> seen;
+        // 1. distinct matrices (same sizes and identical col_ptr / row_idx / val). Instances passing the very arrays
+        //    of an earlier one share its matrix at once; otherwise a matrix is compared (FNV-1a hash, then bytes)
+        //    only with the earlier distinct matrices of the same sizes, and hashed only when there are some.
         std::map<std::tuple<const void*, const void*, const void*, int, int>, int> same_arrays;
+        std::map<std::tuple<int, int, int64_t>, std::vector<int>> by_size;  // (m, n, nnz) -> distinct matrices
+        std::vector<uint64_t> mat_hash;
+        std::vector<char> mat_hashed;
+        auto hash_of = [](const taral_model& m) {
+            const int64_t nz = m.col_ptr[m.n];
+            uint64_t h = 1469598103934665603ull;
+            h = fnv(m.col_ptr, size_t(m.n + 1) * sizeof(int64_t), h);
+            h = fnv(m.row_idx, size_t(nz) * sizeof(int32_t), h);
+            return fnv(m.val, size_t(nz) * sizeof(double), h);
+        };
         mat_of.resize(count);
         for (int i = 0; i < count; ++i) {
             const taral_model& m = md[i];
-            int64_t nz = m.col_ptr[m.n];
+            const int64_t nz = m.col_ptr[m.n];
             const auto akey = std::make_tuple((const void*)m.col_ptr, (const void*)m.row_idx, (const void*)m.val, m.m, m.n);
             auto sa = same_arrays.find(akey);
             if (sa != same_arrays.end()) {  // the very arrays of an earlier instance: the same matrix
                 mat_of[i] = sa->second;
                 continue;
             }
-            uint64_t h = 1469598103934665603ull;
-            h = fnv(m.col_ptr, size_t(m.n + 1) * sizeof(int64_t), h);
-            h = fnv(m.row_idx, size_t(nz) * sizeof(int32_t), h);
-            h = fnv(m.val, size_t(nz) * sizeof(double), h);
-            auto key = std::make_pair(h, std::make_pair(m.m, m.n));
-            auto it = seen.find(key);
-            bool same = false;
-            if (it != seen.end()) {  // confirm byte equality against the first instance with this hash
-                const taral_model& r = md[first_inst[it->second]];
-                same = r.m == m.m && r.n == m.n && r.col_ptr[r.n] == nz &&
-                       !std::memcmp(r.col_ptr, m.col_ptr, size_t(m.n + 1) * sizeof(int64_t)) &&
-                       !std::memcmp(r.row_idx, m.row_idx, size_t(nz) * sizeof(int32_t)) &&
-                       !std::memcmp(r.val, m.val, size_t(nz) * sizeof(double));
+            std::vector<int>& ids = by_size[std::make_tuple(m.m, m.n, nz)];
+            int found = -1;
+            if (!ids.empty()) {
+                const uint64_t h = hash_of(m);
+                for (int id : ids) {
+                    const taral_model& r = md[first_inst[id]];
+                    if (!mat_hashed[id]) mat_hash[id] = hash_of(r), mat_hashed[id] = 1;
+                    if (mat_hash[id] == h && !std::memcmp(r.col_ptr, m.col_ptr, size_t(m.n + 1) * sizeof(int64_t)) &&
+                        !std::memcmp(r.row_idx, m.row_idx, size_t(nz) * sizeof(int32_t)) &&
+                        !std::memcmp(r.val, m.val, size_t(nz) * sizeof(double))) {
+                        found = id;
+                        break;
+                    }
+                }
             }
-            if (same) {
-                mat_of[i] = it->second;
-            } else {
-                int id = int(mats.size());
+            if (found < 0) {
+                found = int(mats.size());
                 mats.push_back(std::make_unique<Shared>());
                 first_inst.push_back(i);
-                if (it == seen.end()) seen[key] = id;
-                mat_of[i] = id;
+                mat_hash.push_back(0), mat_hashed.push_back(0);
+                ids.push_back(found);
             }
-            same_arrays[akey] = mat_of[i];
+            mat_of[i] = found;
+            same_arrays[akey] = found;
         }
         distinct = int(mats.size());
         mark("match");
@@ -802,7 +813,7 @@ struct Batch final : BatchBase {
         A_ev = put(a_ev), Ae_ev = put(ae_ev), T_ev = put(t_ev), Te_ev = put(te_ev);
         rr = put(hrr), cr = put(hcr);
         std::vector<T> hc(N, T(0)), hl(N, T(0)), hu(N, T(0)), hDc(N, T(1)), hrl(M, T(0)), hru(M, T(0)), hDr(M, T(1));
-        for (int i = 0; i < count; ++i) {
+        par_for(count, [&](int i) {  // every instance fills its own slots
             const Scaled& v = vecs[i];
             const Shared& sh = *mats[mat_of[i]];
             for (int j = 0; j < md[i].n; ++j) {
@@ -813,7 +824,7 @@ struct Batch final : BatchBase {
                 const int g = zidx(i, r);
                 hrl[g] = T(v.rl[r]), hru[g] = T(v.ru[r]), hDr[g] = T(sh.S.Dr[r]);
             }
-        }
+        });
         c = put(hc), l = put(hl), u = put(hu), Dc = put(hDc), rl = put(hrl), ru = put(hru), Dr = put(hDr);
         x = alloc<T>(N), ATz = alloc<T>(N), xlast = alloc<T>(N), z = alloc<T>(M), Ax = alloc<T>(M), zlast = alloc<T>(M);
         pv = alloc<T>(N), pu = alloc<T>(N), pw = alloc<T>(M);

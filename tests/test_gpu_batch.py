@@ -33,6 +33,30 @@ def test_batch_of_distinct_models_fp64(engine_lib):
         assert len(x) == lp.n
 
 
+def test_batch_matches_matrices_by_content(engine_lib):
+    """Instances whose matrices are equal but held in separate arrays share one stored matrix; a matrix of the same
+    sizes with one value changed is stored apart; each instance solves as it does alone."""
+    import dataclasses
+    base = lpgen.RefineryBase(2, seed=12)
+    pert = lpgen.perturbations(3, seed=3)
+    a = base.instance(2, pert[0])
+    b = dataclasses.replace(base.instance(2, pert[1]), col_ptr=a.col_ptr.copy(), row_idx=a.row_idx.copy(),
+                            val=a.val.copy())
+    c0 = base.instance(2, pert[2])
+    v = c0.val.copy()
+    v[len(v) // 2] *= 1.5
+    c = dataclasses.replace(c0, val=v)
+    lps = [a, b, c]
+    bt = pdhg.Batch(lps, tol=1e-6, precision=pdhg.FP64, time_limit=300)
+    info = bt.info()
+    assert info["distinct_matrices"] == 2 and info["nnz_stored"] == 2 * len(a.val)
+    res, xs, _ = bt.solve()
+    for lp, r, x in zip(lps, res, xs):
+        s, xs1, _ = pdhg.solve(lp, tol=1e-6, precision=pdhg.FP64)
+        assert r["status"] == s["status"] == "near_optimal"
+        assert abs(r["iterations"] - s["iterations"]) <= 64 and rel(r["objective"], s["objective"]) < 1e-7
+
+
 def test_batch_shares_matrices_fp32(engine_lib):
     base = lpgen.RefineryBase(3, seed=11)
     pert = lpgen.perturbations(5, seed=2)
