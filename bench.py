@@ -39,6 +39,9 @@ region, and the number of engine kernels launched in it.
   python bench.py --workload family --profile-blocks B       ncu capture mode of the batched engine (16 scenarios)
   python bench.py --workload warmstart [--train 512]         the learned warm start on the 24-period family
   python bench.py --workload gemm                            the tcgen05 GEMM's TFLOP/s on the MLP's shapes
+  python bench.py --workload seeds                           the small planted LP (seeds 0-9) and the bench LP
+                                                             (seeds 0-2) on both engines, the reference's CPU IPM,
+                                                             dual simplex and PDHG included
 """
 import argparse
 import json
@@ -143,6 +146,24 @@ def ref_binary():
     return ROOT / "oracle" / "_ref" / "pdhg"
 
 
+def ref_cpu_solver(lp, method, cap_s):
+    """One run of the reference's single-threaded CPU engine `method` ("ipm" or "dual": `oracle/_ref/taral --method`)
+    on the LP, capped at cap_s seconds: wall seconds, status and the objective's error against the planted optimum."""
+    taral = ROOT / "oracle" / "_ref" / "taral"
+    with tempfile.TemporaryDirectory() as td:
+        f, j = Path(td) / "p.mps", Path(td) / "p.json"
+        lp.write_mps(f)
+        t0 = time.perf_counter()
+        try:
+            subprocess.run([str(taral), str(f), "--method", method, "--time-limit", str(cap_s), "--json", str(j)],
+                           check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL, timeout=cap_s + 60)
+            rep = json.loads(j.read_text())
+            return {"s": time.perf_counter() - t0, "status": rep.get("status"),
+                    "objective_rel_err": abs(rep["objective"] - lp.obj_star) / abs(lp.obj_star)}
+        except (subprocess.SubprocessError, OSError, ValueError, KeyError) as e:
+            return {"s": time.perf_counter() - t0, "status": f"failed: {type(e).__name__}"}
+
+
 def cpu_solvers(cap_s=120.0, with_engine=True):
     """The reference's own CPU dual simplex and IPM (single-threaded engines of `oracle/_ref/taral`, each capped at
     cap_s seconds) and this engine on the small planted LP (2,000 x 5,000, 5 nonzeros per column, seed 1), timed
@@ -154,19 +175,8 @@ def cpu_solvers(cap_s=120.0, with_engine=True):
     lp = lpgen.planted(2000, 5000, 5, seed=1)
     out = {"workload": "planted LP m=2000 n=5000, 5 nonzeros per column, seed 1, tol 1e-6", "cores": 1,
            "cap_s": cap_s, "planted_objective": lp.obj_star}
-    with tempfile.TemporaryDirectory() as td:
-        f, j = Path(td) / "p.mps", Path(td) / "p.json"
-        lp.write_mps(f)
-        for method in ("ipm", "dual"):
-            t0 = time.perf_counter()
-            try:
-                subprocess.run([str(taral), str(f), "--method", method, "--time-limit", str(cap_s), "--json", str(j)],
-                               check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL, timeout=cap_s + 60)
-                rep = json.loads(j.read_text())
-                out[method] = {"s": time.perf_counter() - t0, "status": rep.get("status"),
-                               "objective_rel_err": abs(rep["objective"] - lp.obj_star) / abs(lp.obj_star)}
-            except (subprocess.SubprocessError, OSError, ValueError, KeyError) as e:
-                out[method] = {"s": time.perf_counter() - t0, "status": f"failed: {type(e).__name__}"}
+    for method in ("ipm", "dual"):
+        out[method] = ref_cpu_solver(lp, method, cap_s)
     if not with_engine:
         return out
     import pdhg
@@ -776,6 +786,71 @@ def gemm_arm(args):
     print(json.dumps({"workload": "gemm", "peak_bf16_tflops": peak, "peak_kind": kind, "rows": rows}))
 
 
+def seeds_arm(args):
+    """`--workload seeds`: every seed the survey names for the two planted configurations, on both engines.
+    * the small planted LP (2,000 x 5,000, 5 nonzeros per column, seeds 0-9): this engine in FP32 and FP64 from host
+      arrays (median of 3 after a warm-up call), the reference's CPU PDHG (FP64, all host threads) and its
+      single-threaded CPU IPM and dual simplex (one process per seed and method, run side by side on the host's
+      cores, capped at --cap seconds), with every objective's error against the planted optimum;
+    * the bench LP (seeds 0-2): this engine in FP32 and FP64 from host arrays and the reference's GPU backend (FP64).
+    Prints one JSON line with the per-seed results and their medians."""
+    import concurrent.futures as cf
+    import lpgen
+    import pdhg
+    tol = WORKLOAD["tol"]
+
+    def ours(lp, prec, reps):
+        pdhg.solve(lp, tol=tol, precision=prec)
+        ts, r = [], None
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            r, _, _ = pdhg.solve(lp, tol=tol, precision=prec)
+            ts.append(time.perf_counter() - t0)
+        return {"s": statistics.median(ts), "status": r["status"], "iterations": r["iterations"],
+                "objective_rel_err": abs(r["objective"] - lp.obj_star) / abs(lp.obj_star)}
+
+    def ref(lp, device):
+        rep = run_reference(lp, device, tol=tol, limit_s=args.cap if device == "cpu" else 900.0)
+        ok = str(rep.get("status", "")).startswith("near")
+        return {"solve_s": rep.get("solve_s"), "total_s": rep.get("total_s"), "status": rep.get("status"),
+                "iterations": rep.get("iterations"),
+                "objective_rel_err": abs(rep["objective"] - lp.obj_star) / abs(lp.obj_star) if ok else None}
+
+    small = [lpgen.planted(2000, 5000, 5, seed=k) for k in range(10)]
+    rows = [{"seed": k, "fp32": ours(lp, pdhg.FP32, 3), "fp64": ours(lp, pdhg.FP64, 3),
+             "ref_cpu_pdhg": ref(lp, "cpu")} for k, lp in enumerate(small)]
+    cores = os.cpu_count() or 1
+    with cf.ThreadPoolExecutor(max_workers=max(1, min(20, cores // 2))) as ex:
+        jobs = {(k, m): ex.submit(ref_cpu_solver, lp, m, args.cap) for k, lp in enumerate(small) for m in ("ipm", "dual")}
+        for (k, m), fut in jobs.items():
+            rows[k]["ref_" + m] = fut.result()
+
+    def med(key, field):
+        v = [r[key][field] for r in rows if r[key].get(field) is not None]
+        return statistics.median(v) if v else None
+
+    small_out = {"workload": "planted LP m=2000 n=5000, 5 nonzeros per column, seeds 0-9, tol 1e-6",
+                 "host_cores": cores, "cap_s": args.cap, "seeds": rows,
+                 "median_s": {"fp32": med("fp32", "s"), "fp64": med("fp64", "s"),
+                              "ref_cpu_pdhg_solve": med("ref_cpu_pdhg", "solve_s"),
+                              "ref_cpu_pdhg_total": med("ref_cpu_pdhg", "total_s"),
+                              "ref_ipm": med("ref_ipm", "s"), "ref_dual": med("ref_dual", "s")},
+                 "how": "this engine: taral_pdhg_solve from host arrays, median of 3; reference PDHG: its own "
+                        "solve_s / total_s; IPM and dual simplex: process wall time, up to "
+                        f"{max(1, min(20, cores // 2))} single-threaded processes side by side"}
+    big = []
+    for k in range(3):
+        lp = make_lp(k)
+        big.append({"seed": k, "m": lp.m, "n": lp.n, "nnz": int(lp.col_ptr[-1]), "fp32": ours(lp, pdhg.FP32, 1),
+                    "fp64": ours(lp, pdhg.FP64, 1), "ref_gpu_backend": ref(lp, "gpu")})
+        del lp
+    print(json.dumps({"workload": "seeds", "metric": METRIC, "unit": "s", "small_lp": small_out,
+                      "bench_lp": {"workload": WORKLOAD_NAME, "seeds": big,
+                                   "how": "this engine: taral_pdhg_solve from host arrays after a warm-up call; "
+                                          "reference: its GPU backend (FP64), its solve_s and total_s"}}),
+          flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -789,10 +864,12 @@ def main():
     ap.add_argument("--no-learned", action="store_true", help="skip the learned warm-start block")
     ap.add_argument("--oracle-sample", type=int, default=4,
                     help="family scenarios given the FP64 objective oracle (0: no oracle, no 48-period LP)")
-    ap.add_argument("--workload", choices=["lp", "family", "warmstart", "ledger", "gemm"], default="lp",
+    ap.add_argument("--workload", choices=["lp", "family", "warmstart", "ledger", "gemm", "seeds"], default="lp",
                     help="lp: the single large LP (the bench line); family: the batched scenario family; "
                          "warmstart: the learned warm start on the 24-period family; ledger: the reference's "
-                         "published PDHG workloads (both arms)")
+                         "published PDHG workloads (both arms); seeds: every seed of the small planted LP and the "
+                         "bench LP on both engines")
+    ap.add_argument("--cap", type=float, default=120.0, help="seconds per reference CPU run in --workload seeds")
     ap.add_argument("--instances", type=int, default=512)
     ap.add_argument("--sample", type=int, default=12)
     ap.add_argument("--train", type=int, default=512)
@@ -811,6 +888,10 @@ def main():
     if args.workload == "gemm":
         if rank == 0:
             gemm_arm(args)
+        return
+    if args.workload == "seeds":
+        if rank == 0:
+            seeds_arm(args)
         return
     if args.workload in ("family", "warmstart"):
         if rank == 0:
