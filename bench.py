@@ -787,7 +787,7 @@ def gemm_arm(args):
 
 
 def seeds_arm(args):
-    """`--workload seeds`: every seed the survey names for the two planted configurations, on both engines.
+    """`--workload seeds`: the two planted LPs over their seeds (small LP 0-9, bench LP 0-2), on both engines.
     * the small planted LP (2,000 x 5,000, 5 nonzeros per column, seeds 0-9): this engine in FP32 and FP64 from host
       arrays (median of 3 after a warm-up call), the reference's CPU PDHG (FP64, all host threads) and its
       single-threaded CPU IPM and dual simplex (one process per seed and method, run side by side on the host's
