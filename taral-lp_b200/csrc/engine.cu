@@ -55,6 +55,31 @@ void keep_pool_memory(int dev) {
     done.push_back(dev);
 }
 
+// Pinned host blocks for the contexts' status reads, kept for the process once allocated: cudaMallocHost and
+// cudaFreeHost cost up to milliseconds per call (and the free synchronises the device), a visible part of a small
+// LP's solve. A block holds 32 doubles and an int.
+constexpr size_t kPinnedBlock = 512;
+static_assert(32 * sizeof(double) + sizeof(int) <= kPinnedBlock, "a status block holds 32 doubles and an int");
+std::mutex g_pinned_mu;
+std::vector<void*> g_pinned_free;
+void* pinned_block() {
+    {
+        std::lock_guard<std::mutex> lock(g_pinned_mu);
+        if (!g_pinned_free.empty()) {
+            void* p = g_pinned_free.back();
+            g_pinned_free.pop_back();
+            return p;
+        }
+    }
+    void* p = nullptr;
+    return cudaMallocHost(&p, kPinnedBlock) == cudaSuccess ? p : nullptr;
+}
+void pinned_return(void* p) {
+    if (!p) return;
+    std::lock_guard<std::mutex> lock(g_pinned_mu);
+    g_pinned_free.push_back(p);
+}
+
 // ---------------------------------------------------------------------------------------------- row blocks
 // Consecutive rows are packed into blocks of at most kTile nonzeros and kRowsMax rows; a longer row is a block of
 // its own (block_sums sums it with the whole CTA).
@@ -392,8 +417,9 @@ struct Engine final : EngineBase {
         tickets = zeros<unsigned>(4);
         pdone = zeros<int>(1);
         hc.assign(hc_ptr, hc_ptr + n), hrl.assign(hrl_ptr, hrl_ptr + m), hru.assign(hru_ptr, hru_ptr + m);
-        CK(cudaMallocHost(&h_out, 32 * sizeof(double)));
-        CK(cudaMallocHost(&h_flag, sizeof(int)));
+        h_out = static_cast<double*>(pinned_block());
+        if (!h_out) throw CudaError{"cudaMallocHost: no pinned host memory for the status reads"};
+        h_flag = reinterpret_cast<int*>(h_out + 32);
         CK(cudaStreamSynchronize(st));
         mem_used = alloc_bytes;
         tune();
@@ -403,8 +429,7 @@ struct Engine final : EngineBase {
         if (graph) cudaGraphExecDestroy(graph);
         for (void* p : allocs) cudaFreeAsync(p, st);  // back to the pool: no device-wide synchronisation
         if (st) cudaStreamSynchronize(st);
-        if (h_out) cudaFreeHost(h_out);
-        if (h_flag) cudaFreeHost(h_flag);
+        pinned_return(h_out);  // after the synchronisation above: no copy into it is in flight
         if (st) cudaStreamDestroy(st);
     }
 
