@@ -27,11 +27,11 @@ Csr transpose_par(const int64_t* ptr, const int32_t* idx, const double* val, int
         cut[q] = int(std::lower_bound(ptr, ptr + rows + 1, ptr[0] + nnz * q / parts) - ptr);
     for (int q = 1; q <= parts; ++q) cut[q] = std::max(cut[q], cut[q - 1]);
     // slot[q][j]: range q's count of output row j, then the offset of its first entry inside that row
-    std::vector<std::vector<int32_t>> slot(static_cast<size_t>(parts));
+    // (allocated here, so that an allocation failure reaches the caller rather than a worker thread)
+    std::vector<std::vector<int32_t>> slot(static_cast<size_t>(parts), std::vector<int32_t>(size_t(cols), 0));
     split_ranges(parts, parts, [&](int, int64_t q0, int64_t q1) {
         for (int64_t q = q0; q < q1; ++q) {
             std::vector<int32_t>& c = slot[size_t(q)];
-            c.assign(size_t(cols), 0);
             for (int64_t k = ptr[cut[q]]; k < ptr[cut[q + 1]]; ++k) c[size_t(idx[k])]++;
         }
     });
