@@ -19,6 +19,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -53,6 +54,20 @@ void keep_pool_memory(int dev) {
         cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
     }
     done.push_back(dev);
+}
+
+// The device's name, queried once per device (the full property query is slow next to a small LP's solve).
+std::string device_name(int dev) {
+    static std::mutex mu;
+    static std::map<int, std::string> names;
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = names.find(dev);
+    if (it != names.end()) return it->second;
+    char buf[256] = {0};
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, dev) == cudaSuccess) std::snprintf(buf, sizeof buf, "%s", prop.name);
+    else cudaGetLastError();
+    return names[dev] = buf;
 }
 
 // Pinned host blocks for the contexts' status reads, kept for the process once allocated: cudaMallocHost and
@@ -224,9 +239,7 @@ struct Engine final : EngineBase {
         int dev;
         CK(cudaGetDevice(&dev));
         keep_pool_memory(dev);
-        cudaDeviceProp prop;
-        CK(cudaGetDeviceProperties(&prop, dev));
-        name = prop.name;
+        name = device_name(dev);
         CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
         if (const char* e = std::getenv("TARAL_PDL")) pdl = std::atoi(e) != 0;
     }
