@@ -188,6 +188,7 @@ struct Engine final : EngineBase {
     int* h_flag = nullptr;
     cudaStream_t st = nullptr;
     cudaGraphExec_t graph = nullptr;
+    cudaGraphExec_t pgraph = nullptr;  // a chunk of power-iteration steps
     std::vector<void*> allocs;
     bool started = false;
 
@@ -440,6 +441,7 @@ struct Engine final : EngineBase {
     ~Engine() override {
         if (ev0) cudaEventDestroy(ev0), cudaEventDestroy(ev1);
         if (graph) cudaGraphExecDestroy(graph);
+        if (pgraph) cudaGraphExecDestroy(pgraph);
         for (void* p : allocs) cudaFreeAsync(p, st);  // back to the pool: no device-wide synchronisation
         if (st) cudaStreamSynchronize(st);
         pinned_return(h_out);  // after the synchronisation above: no copy into it is in flight
@@ -589,18 +591,36 @@ struct Engine final : EngineBase {
         CK(cudaMemsetAsync(pdone, 0, sizeof(int), st));
         launches += 1;
         T *a = pv, *b = pu;
-        const int chunk = 8;  // steps queued between checks of the device-side stop flag
+        // steps queued between checks of the device-side stop flag; an even count, so that every chunk starts with
+        // the vectors in the same roles and a chunk captured once replays as a CUDA graph
+        const int chunk = 8;
+        auto step = [&] {
+            spmv(A, a, pw, pdone);
+            spmv(AT, pw, b, pdone);
+            k_power_sumsq<T><<<red_grid(n), kRedThreads, 0, st>>>(n, b, part, tickets + 2, out + 24, pdone);
+            k_power_update<<<1, 1, 0, st>>>(out + 24, pst, pdone);
+            k_power_scale<T><<<grid_for(n), 256, 0, st>>>(n, b, pst, pdone);
+            launches += 3;
+            std::swap(a, b);
+        };
         for (int it = 0; it < iters;) {
-            int end = std::min(iters, it + chunk);
-            for (; it < end; ++it) {
-                spmv(A, a, pw, pdone);
-                spmv(AT, pw, b, pdone);
-                int g = red_grid(n);
-                k_power_sumsq<T><<<g, kRedThreads, 0, st>>>(n, b, part, tickets + 2, out + 24, pdone);
-                k_power_update<<<1, 1, 0, st>>>(out + 24, pst, pdone, it);
-                k_power_scale<T><<<grid_for(n), 256, 0, st>>>(n, b, pst, pdone);
-                launches += 3;
-                std::swap(a, b);
+            const int end = std::min(iters, it + chunk);
+            if (use_graph && end - it == chunk) {
+                if (!pgraph) {  // capturing swaps a and b `chunk` times: they end in their starting roles
+                    const int64_t before = launches;
+                    cudaGraph_t g;
+                    CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+                    for (int k = 0; k < chunk; ++k) step();
+                    CK(cudaStreamEndCapture(st, &g));
+                    CK(cudaGraphInstantiate(&pgraph, g, 0));
+                    CK(cudaGraphDestroy(g));
+                    launches = before;
+                }
+                CK(cudaGraphLaunch(pgraph, st));
+                launches += 5 * chunk;  // two SpMVs and three small kernels per step
+                it = end;
+            } else {
+                for (; it < end; ++it) step();
             }
             CK(cudaMemcpyAsync(h_flag, pdone, sizeof(int), cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));

@@ -702,7 +702,8 @@ __global__ void __launch_bounds__(kRedThreads) k_eval_col(int n, double f, const
     reduce_finish<5>(v, part, ticket, out);
 }
 
-// Power iteration on A_s^T A_s with the stop test on the device (gpu/pdhg.cu:425-434). st = {est, prev, scale};
+// Power iteration on A_s^T A_s with the stop test on the device (gpu/pdhg.cu:425-434). st = {est, prev, scale,
+// steps taken} (the step count lives on the device, so that a captured chunk of steps can be replayed);
 // *done is set once the estimate has converged (after step 10, |est - prev| <= 1e-7 est) or when ||v||^2 <= 0,
 // and every later kernel of the queued steps returns at once.
 template <class T>
@@ -714,9 +715,10 @@ __global__ void __launch_bounds__(kRedThreads) k_power_sumsq(int n, const T* __r
     reduce_finish<1>(a, part, ticket, out);
 }
 
-static __global__ void k_power_update(const double* out, double* st, int* done, int it) {  // one thread
+static __global__ void k_power_update(const double* out, double* st, int* done) {  // one thread
     if (*done) return;
-    double s = out[0], prev = st[0];
+    const double s = out[0], prev = st[0], it = st[3];
+    st[3] = it + 1;
     if (s <= 0) { st[0] = 0, *done = 1; return; }
     double est = sqrt(sqrt(s));
     st[0] = est, st[1] = prev, st[2] = 1 / sqrt(s);
