@@ -252,3 +252,23 @@ def test_programmatic_launch_changes_nothing(engine_lib, oracle_lib, monkeypatch
     (c0, a0), (x0, z0) = outs[0]
     (c1, a1), (x1, z1) = outs[1]
     assert np.array_equal(c0, c1) and np.array_equal(a0, a1) and np.array_equal(x0, x1) and np.array_equal(z0, z1)
+
+
+@pytest.mark.parametrize("precision", [pdhg.FP64, pdhg.FP32], ids=["fp64", "fp32"])
+def test_power_norm_replay_and_repeated_solves(engine_lib, oracle_lib, precision):
+    """The power iteration replays one captured chunk of steps: a second call on the same context and a context
+    without graphs give the same estimate (FP64: the oracle's to 1e-12); two solves on one context give the same
+    outcome and point."""
+    lp = CASES["planted_zipf"]()
+    sp = oracle.ScaledProblem(lp)
+    eng = pdhg.Engine.from_scaled(sp, precision=precision)
+    direct = pdhg.Engine.from_scaled(sp, precision=precision, graph=False)
+    a, b, c = eng.power_norm(200), eng.power_norm(200), direct.power_norm(200)
+    assert a == b == c, (a, b, c)
+    if precision == pdhg.FP64:
+        assert abs(a - sp.power_norm(200)) <= 1e-12 * a
+    e2 = pdhg.Engine.from_model(lp, precision=precision)
+    (r0, x0, z0), (r1, x1, z1) = [e2.solve(e2.bnorm, e2.cnorm, tol=1e-6) for _ in range(2)]
+    assert r0["status"] == r1["status"] == "near_optimal"
+    assert (r0["iterations"], r0["restarts"], r0["objective"]) == (r1["iterations"], r1["restarts"], r1["objective"])
+    assert np.array_equal(x0, x1) and np.array_equal(z0, z1)
